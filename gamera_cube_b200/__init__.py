@@ -1,0 +1,82 @@
+"""Python host interface of libgamera_cs_b200 (the B200 cubed-sphere MHD
+step and ionosphere solve).
+
+The shared library is built in place (``make -C gamera_cube_b200``); importing
+this package loads it and raises if it is missing: there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libgamera_cs_b200.so")
+
+
+def _load():
+    if not os.path.exists(LIBRARY_PATH):
+        raise ImportError(
+            "libgamera_cs_b200.so is not built (run make -C gamera_cube_b200); "
+            "the CUDA library is required, there is no CPU fallback")
+    lib = C.CDLL(LIBRARY_PATH, mode=os.RTLD_LOCAL | getattr(os, "RTLD_NOW", 2))
+    P = C.POINTER
+    c_sz3 = C.c_size_t * 3
+    sig = {
+        "gamera_cs_advance_six": (C.c_int, [P(abi.Grid), P(abi.Storage), c_sz3,
+                                            C.c_size_t, C.c_double, C.c_double,
+                                            P(abi.AdvanceOptions)]),
+        "gamera_cs_advance_six_with_background_planned": (
+            C.c_int, [P(abi.Grid), P(abi.Storage), c_sz3, C.c_size_t, C.c_double,
+                      C.c_double, P(abi.AdvanceOptions), P(abi.BackgroundField),
+                      C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
+        "gamera_cs_halo_plan_create": (C.c_int, [P(abi.Grid), c_sz3, C.c_size_t,
+                                                 P(C.c_void_p)]),
+        "gamera_cs_halo_plan_destroy": (None, [C.c_void_p]),
+        "gamera_cs_fill_tangential_cell_halos_planned": (
+            C.c_int, [C.c_void_p, P(abi.Grid), P(abi.Storage)]),
+        "gamera_cs_fill_magnetic_face_halos_planned": (
+            C.c_int, [C.c_void_p, P(abi.Grid), P(abi.Storage)]),
+        "gamera_cs_halo_valid_state": (C.c_int, [P(C.c_double)]),
+        "gcs_context_create": (C.c_void_p, [P(abi.Grid), c_sz3, C.c_size_t]),
+        "gcs_context_destroy": (None, [C.c_void_p]),
+        "gcs_last_error": (C.c_char_p, []),
+        "gcs_context_error": (C.c_char_p, [C.c_void_p]),
+        "gcs_context_upload_background": (C.c_int, [C.c_void_p,
+                                                    P(abi.BackgroundField)]),
+        "gcs_context_upload_state": (C.c_int, [C.c_void_p, P(abi.Storage)]),
+        "gcs_context_download_state": (C.c_int, [C.c_void_p, P(abi.Storage),
+                                                 C.c_int]),
+        "gcs_context_step": (C.c_int, [C.c_void_p, P(abi.AdvanceOptions),
+                                       C.c_double, C.c_double]),
+        "gcs_context_timestep": (C.c_int, [C.c_void_p, P(abi.TimestepOptions),
+                                           P(C.c_double)]),
+        "gcs_context_run": (C.c_int, [C.c_void_p, P(abi.AdvanceOptions),
+                                      P(abi.TimestepOptions), C.c_double,
+                                      C.c_int, C.c_int]),
+        "gcs_context_sync": (C.c_int, [C.c_void_p]),
+        "gcs_context_params": (C.c_int, [C.c_void_p, P(C.c_double),
+                                         P(C.c_double), P(C.c_double),
+                                         P(C.c_int)]),
+        "gcs_context_set_params": (C.c_int, [C.c_void_p, C.c_double, C.c_double,
+                                             C.c_double, C.c_int]),
+        "gcs_context_failure": (C.c_int, [C.c_void_p] + [P(C.c_int)] * 5),
+        "gcs_context_reset_failure": (C.c_int, [C.c_void_p]),
+        "gcs_context_stream": (C.c_size_t, [C.c_void_p]),
+        "gcs_context_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+        "gcs_context_stage_times": (C.c_int, [C.c_void_p, P(C.c_double),
+                                              P(C.c_longlong), C.c_int]),
+        "gcs_stage_name": (C.c_char_p, [C.c_int]),
+        "gcs_context_device_bytes": (C.c_size_t, [C.c_void_p]),
+        "gcs_halo_plan_context": (C.c_void_p, [C.c_void_p]),
+        "gcs_context_set_resident": (C.c_int, [C.c_void_p, C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+__all__ = ["abi", "lib", "LIBRARY_PATH"]

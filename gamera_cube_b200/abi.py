@@ -1,0 +1,184 @@
+"""ctypes mirrors of the reference GAMERA-Cube C data types.
+
+Layout-identical to include/gamera_cs_types.h (and therefore to the
+reference headers cited there); used by the Python host interface and the
+tests to hand reference-layout host arrays to the C-ABI library.
+"""
+import ctypes as C
+
+import numpy as np
+
+FACE_COUNT = 6
+FLUX_COUNT = 5
+
+
+class Vec3(C.Structure):
+    _fields_ = [("value", C.c_double * 3)]
+
+
+class FaceGeometry(C.Structure):
+    _fields_ = [("area", C.c_double), ("area_vector", Vec3), ("centroid", Vec3),
+                ("normal", Vec3), ("tangent1", Vec3), ("tangent2", Vec3)]
+
+
+class CellGeometry(C.Structure):
+    _fields_ = [("volume", C.c_double), ("centroid", Vec3),
+                ("face", (FaceGeometry * 2) * 3), ("cfl_length", C.c_double * 3)]
+
+
+class EdgeGeometry(C.Structure):
+    _fields_ = [("length", C.c_double), ("normal", Vec3), ("tangent1", Vec3),
+                ("tangent2", Vec3)]
+
+
+class FaceGrid(C.Structure):
+    _fields_ = [("extent", C.c_size_t * 3), ("value", C.POINTER(FaceGeometry))]
+
+
+class EdgeGrid(C.Structure):
+    _fields_ = [("extent", C.c_size_t * 3), ("value", C.POINTER(EdgeGeometry)),
+                ("valid", C.POINTER(C.c_ubyte))]
+
+
+class Grid(C.Structure):
+    _fields_ = [("cell_extent", C.c_size_t * 3), ("vertex_extent", C.c_size_t * 3),
+                ("vertex", C.POINTER(Vec3)), ("cell", C.POINTER(CellGeometry)),
+                ("face", FaceGrid * 3), ("edge", EdgeGrid * 3)]
+
+
+class Storage(C.Structure):
+    _fields_ = [
+        ("cell_extent", C.c_size_t * 3),
+        ("face_extent", (C.c_size_t * 3) * 3),
+        ("edge_extent", (C.c_size_t * 3) * 3),
+        ("conserved", C.POINTER(C.c_double)),
+        ("old_conserved", C.POINTER(C.c_double)),
+        ("predicted_conserved", C.POINTER(C.c_double)),
+        ("cell_magnetic", C.POINTER(Vec3)),
+        ("old_cell_magnetic", C.POINTER(Vec3)),
+        ("predicted_cell_magnetic", C.POINTER(Vec3)),
+        ("face_flux", C.POINTER(C.c_double) * 3),
+        ("old_face_flux", C.POINTER(C.c_double) * 3),
+        ("predicted_face_flux", C.POINTER(C.c_double) * 3),
+        ("edge_emf", C.POINTER(C.c_double) * 3),
+        ("fluid_face_flux", C.POINTER(C.c_double) * 3),
+        ("maxwell_face_flux", C.POINTER(Vec3) * 3),
+        ("hydro_rate", C.POINTER(C.c_double)),
+        ("maxwell_rate", C.POINTER(Vec3)),
+        ("emergency_diffusion_face_count", C.c_size_t),
+        ("emergency_diffusion_max_interface_speed", C.c_double),
+        ("inner_wall_clamped_face_count", C.c_size_t * 2),
+        ("inner_wall_positive_mass_max", C.c_double * 2),
+        ("inner_wall_positive_energy_max", C.c_double * 2),
+        ("inner_wall_fluid_momentum_max", C.c_double * 2),
+        ("inner_wall_maxwell_momentum_max", C.c_double * 2),
+        ("inner_wall_density_max", C.c_double * 2),
+        ("inner_wall_pressure_max", C.c_double * 2),
+        ("inner_wall_pressure_gradient_max", C.c_double * 2),
+        ("inner_wall_speed_max", C.c_double * 2),
+        ("inner_wall_residual_magnetic_max", C.c_double * 2),
+        ("inner_wall_residual_magnetic_location", Vec3 * 2),
+        ("inner_wall_lowlat_pressure_max", C.c_double * 2),
+        ("inner_wall_lowlat_pressure_gradient_max", C.c_double * 2),
+        ("inner_wall_lowlat_speed_max", C.c_double * 2),
+        ("inner_wall_lowlat_residual_magnetic_max", C.c_double * 2),
+    ]
+
+
+class SweepOptions(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("density_floor", C.c_double),
+                ("pressure_floor", C.c_double), ("pdm_coefficient", C.c_double),
+                ("hydro_hogs_coefficient", C.c_double),
+                ("magnetic_hogs_coefficient", C.c_double),
+                ("light_speed", C.c_double), ("use_mhd", C.c_bool),
+                ("use_hogs", C.c_bool), ("use_boris", C.c_bool),
+                ("use_background", C.c_bool)]
+
+
+class BackgroundField(C.Structure):
+    _fields_ = [("cell_magnetic", C.POINTER(Vec3)),
+                ("face_magnetic", C.POINTER(Vec3) * 3),
+                ("face_flux", C.POINTER(C.c_double) * 3),
+                ("edge_magnetic", C.POINTER(Vec3) * 3),
+                ("cell_force", C.POINTER(Vec3))]
+
+
+class EmfOptions(C.Structure):
+    _fields_ = [("density_floor", C.c_double), ("pdm_coefficient", C.c_double),
+                ("diffusion_coefficient", C.c_double), ("light_speed", C.c_double),
+                ("cfl", C.c_double), ("dt", C.c_double), ("use_boris", C.c_bool),
+                ("use_background", C.c_bool)]
+
+
+class UpdateOptions(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("density_floor", C.c_double),
+                ("pressure_floor", C.c_double), ("light_speed", C.c_double),
+                ("use_mhd", C.c_bool), ("use_boris", C.c_bool),
+                ("use_background", C.c_bool)]
+
+
+class TimestepOptions(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("density_floor", C.c_double),
+                ("pressure_floor", C.c_double), ("cfl", C.c_double),
+                ("light_speed", C.c_double), ("use_mhd", C.c_bool),
+                ("use_boris", C.c_bool), ("use_background", C.c_bool)]
+
+
+class AdvanceOptions(C.Structure):
+    _fields_ = [("stress", SweepOptions), ("emf", EmfOptions),
+                ("update", UpdateOptions), ("cell_source", C.c_void_p),
+                ("source_context", C.c_void_p), ("indexed_cell_source", C.c_void_p),
+                ("indexed_source_context", C.c_void_p), ("source_time", C.c_double),
+                ("fluid_flux_sync", C.c_void_p), ("fluid_flux_context", C.c_void_p),
+                ("edge_emf_sync", C.c_void_p), ("edge_emf_context", C.c_void_p)]
+
+
+class MiSolverConfig(C.Structure):
+    _fields_ = [("longitude_count", C.c_size_t), ("colatitude_count", C.c_size_t),
+                ("maximum_colatitude", C.c_double),
+                ("ionosphere_radius_m", C.c_double),
+                ("pedersen_siemens", C.c_double), ("hall_siemens", C.c_double),
+                ("low_latitude_potential_v", C.c_double), ("hemisphere", C.c_int),
+                ("maximum_iterations", C.c_int), ("relative_tolerance", C.c_double),
+                ("absolute_tolerance", C.c_double)]
+
+
+class MiSolverStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("initial_residual", C.c_double),
+                ("final_residual", C.c_double), ("converged", C.c_int)]
+
+
+def _view(ptr, count):
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_double)), shape=(count,))
+
+
+def storage_arrays(storage):
+    """numpy views (no copy) of the arrays of one gamera_no_storage."""
+    ce = tuple(storage.cell_extent)
+    ncell = ce[0] * ce[1] * ce[2]
+    out = {
+        "conserved": _view(storage.conserved, 5 * ncell).reshape(ce + (5,)),
+        "old_conserved": _view(storage.old_conserved, 5 * ncell).reshape(ce + (5,)),
+        "predicted_conserved":
+            _view(storage.predicted_conserved, 5 * ncell).reshape(ce + (5,)),
+        "cell_magnetic": _view(storage.cell_magnetic, 3 * ncell).reshape(ce + (3,)),
+        "old_cell_magnetic":
+            _view(storage.old_cell_magnetic, 3 * ncell).reshape(ce + (3,)),
+        "predicted_cell_magnetic":
+            _view(storage.predicted_cell_magnetic, 3 * ncell).reshape(ce + (3,)),
+    }
+    for d in range(3):
+        fe = tuple(storage.face_extent[d])
+        ee = tuple(storage.edge_extent[d])
+        nf = fe[0] * fe[1] * fe[2]
+        ne = ee[0] * ee[1] * ee[2]
+        out["face_flux%d" % d] = _view(storage.face_flux[d], nf).reshape(fe)
+        out["old_face_flux%d" % d] = _view(storage.old_face_flux[d], nf).reshape(fe)
+        out["predicted_face_flux%d" % d] = \
+            _view(storage.predicted_face_flux[d], nf).reshape(fe)
+        out["fluid_face_flux%d" % d] = \
+            _view(storage.fluid_face_flux[d], 5 * nf).reshape(fe + (5,))
+        out["maxwell_face_flux%d" % d] = \
+            _view(storage.maxwell_face_flux[d], 3 * nf).reshape(fe + (3,))
+        out["edge_emf%d" % d] = _view(storage.edge_emf[d], ne).reshape(ee)
+    return out

@@ -1,0 +1,68 @@
+// Host-side owner of one six-face device run: device arrays, plans, stream,
+// optional CUDA graph of the driver step, and the state transfers between
+// the caller's reference-layout host arrays and the device node layout.
+#pragma once
+
+#include <cstdio>
+
+#include "gamera_cs_types.h"
+#include "gcs_kernels.cuh"
+
+namespace gcs {
+
+enum ArrayKind {
+  kArrU, kArrUo, kArrUp, kArrB, kArrBo, kArrBp,
+  kArrP, kArrPo, kArrPp, kArrF, kArrM, kArrE
+};
+
+struct Context {
+  Ctx X;
+  cudaStream_t stream = nullptr;
+  void *pool = nullptr;
+  size_t pool_bytes = 0;
+  void *bg_pool = nullptr;
+  size_t bg_bytes = 0;
+  void *plans = nullptr;
+  size_t plans_bytes = 0;
+  void *staging = nullptr;
+  size_t staging_bytes = 0;
+  void *staging_host = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  unsigned long long graph_key = 0;
+  int bg_uploaded = 0;
+  const void *bg_key[kFaces][11] = {};
+  const gamera_no_cell_geometry *grid_cell[kFaces] = {};
+  const gamera_no_face_geometry *grid_face[kFaces][3] = {};
+  // device state belongs to this host storage (resident mode)
+  const gamera_no_storage *resident_storage = nullptr;
+  int resident = 0;
+  DevStatus host_status{};
+  char error[256] = {0};
+  // per-stage timing (profiling mode)
+  int profiling = 0;
+  double stage_ms[16] = {0};
+  long long stage_calls[16] = {0};
+
+  ~Context();
+  int init(const gamera_no_grid grid[kFaces], const size_t active[3],
+           size_t ghost);
+  void release();
+  int upload_background(const gamera_no_background_field bg[kFaces]);
+  bool background_matches(const gamera_no_background_field bg[kFaces]) const;
+  int transfer_array(int f, int kind, int dir, bool upload, double *host);
+  int upload_state(const gamera_no_storage st[kFaces]);
+  int download_state(gamera_no_storage st[kFaces], int scratch);
+  void reset_status_async();
+  int read_status(DevStatus *out);
+  void set_error(const char *what, const char *where);
+  bool grid_matches(const gamera_no_grid grid[kFaces]) const {
+    for (int f = 0; f < kFaces; ++f) {
+      if (grid[f].cell != grid_cell[f]) return false;
+      for (int d = 0; d < 3; ++d)
+        if (grid[f].face[d].value != grid_face[f][d]) return false;
+    }
+    return true;
+  }
+};
+
+}  // namespace gcs

@@ -1,0 +1,45 @@
+// Device context of one six-face cubed-sphere run and the stage launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gcs_device.cuh"
+
+namespace gcs {
+
+struct Ctx {
+  Dims D;
+  DevState S;
+  DevGeom G;
+  DevBg BG;
+  Seam *seams = nullptr;
+  HaloCell *halo_cells = nullptr;
+  long long n_halo_cells = 0;
+  HaloFace *halo_faces = nullptr;
+  long long n_halo_faces = 0;
+  int *edge_offsets = nullptr;
+  EdgeMember *edge_members = nullptr;
+  int n_edge_groups = 0;
+  StepParams *params = nullptr;   // device
+  DevStatus *status = nullptr;    // device
+};
+
+void launch_seam_sync(const Ctx &X, int magnetic, cudaStream_t s);
+void launch_halo(const Ctx &X, cudaStream_t s);
+void launch_halo_cells_only(const Ctx &X, cudaStream_t s);
+void launch_halo_faces_only(const Ctx &X, cudaStream_t s);
+void launch_predict(const Ctx &X, const Opts &O, cudaStream_t s);
+void launch_flux(const Ctx &X, const Opts &O, cudaStream_t s);
+void launch_emf(const Ctx &X, const Opts &O, cudaStream_t s);
+void launch_edge_sync(const Ctx &X, cudaStream_t s);
+void launch_update(const Ctx &X, const Opts &O, cudaStream_t s);
+void launch_recover(const Ctx &X, const Opts &O, int with_cfl,
+                    cudaStream_t s);
+void launch_next_dt(const Ctx &X, double fraction, cudaStream_t s);
+void launch_count_step(const Ctx &X, cudaStream_t s);
+void launch_step(const Ctx &X, const Opts &O, int driver_mode,
+                 cudaStream_t s);
+// CFL reduction alone (nonorthogonal_step.c:449-525) into status.
+void launch_timestep(const Ctx &X, const Opts &O, cudaStream_t s);
+
+}  // namespace gcs

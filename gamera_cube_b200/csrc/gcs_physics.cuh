@@ -1,0 +1,441 @@
+// Device-side MHD point operators of the cubed-sphere step.
+//
+// Every function restates one reference operator with the same operation
+// order (so the FP64 path tracks the CPU reference to round-off); the cited
+// lines are in the GAMERA-Cube project.  Functions return 0 on success and a
+// nonzero value where the reference returns -1.
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+
+namespace gcs {
+
+struct Prim {
+  double rho, vx, vy, vz, p;
+};
+
+__host__ __device__ inline double dot3(double ax, double ay, double az,
+                                       double bx, double by, double bz) {
+  // nonorthogonal_flux.c:9-15.  The sum starts at +0.0 as in the
+  // reference, so a product of -0.0 yields the same +0.0 result.
+  double r = 0.0;
+  r += ax * bx;
+  r += ay * by;
+  r += az * bz;
+  return r;
+}
+
+// nonorthogonal_reconstruction.c:7-9, 19-26, 53-55
+__host__ __device__ inline double central8(const double s[8]) {
+  double r = 0.0;
+  r += (-3.0 / 840.0) * s[0];
+  r += (29.0 / 840.0) * s[1];
+  r += (-139.0 / 840.0) * s[2];
+  r += (533.0 / 840.0) * s[3];
+  r += (533.0 / 840.0) * s[4];
+  r += (-139.0 / 840.0) * s[5];
+  r += (29.0 / 840.0) * s[6];
+  r += (-3.0 / 840.0) * s[7];
+  return r;
+}
+
+// nonorthogonal_reconstruction.c:11-13, 57-59
+__host__ __device__ inline double central6(const double s[8]) {
+  double r = 0.0;
+  r += (0.0) * s[0];
+  r += (1.0 / 60.0) * s[1];
+  r += (-8.0 / 60.0) * s[2];
+  r += (37.0 / 60.0) * s[3];
+  r += (37.0 / 60.0) * s[4];
+  r += (-8.0 / 60.0) * s[5];
+  r += (1.0 / 60.0) * s[6];
+  r += (0.0) * s[7];
+  return r;
+}
+
+// nonorthogonal_reconstruction.c:15-17, 28-34
+__host__ __device__ inline double upwind7_left(const double w[8]) {
+  double r = 0.0;
+  r += (-3.0 / 420.0) * w[0];
+  r += (25.0 / 420.0) * w[1];
+  r += (-101.0 / 420.0) * w[2];
+  r += (319.0 / 420.0) * w[3];
+  r += (214.0 / 420.0) * w[4];
+  r += (-38.0 / 420.0) * w[5];
+  r += (4.0 / 420.0) * w[6];
+  return r;
+}
+__host__ __device__ inline double upwind7_right(const double w[8]) {
+  double r = 0.0;
+  r += (-3.0 / 420.0) * w[7];
+  r += (25.0 / 420.0) * w[6];
+  r += (-101.0 / 420.0) * w[5];
+  r += (319.0 / 420.0) * w[4];
+  r += (214.0 / 420.0) * w[3];
+  r += (-38.0 / 420.0) * w[2];
+  r += (4.0 / 420.0) * w[1];
+  return r;
+}
+
+// nonorthogonal_reconstruction.c:36-51 (Fortran SIGN(1,x) == copysign)
+__host__ __device__ inline double pdm_left(double q0, double q1, double q2,
+                                           double interpolated, double pdmb) {
+  const double bounded = fmax(fmin(q1, q2), fmin(interpolated, fmax(q1, q2)));
+  const double delta0 = pdmb * (q1 - q0);
+  const double delta1 = pdmb * (q2 - q1);
+  const double sign0 = copysign(1.0, delta0);
+  const double sign1 = copysign(1.0, delta1);
+  const double same = fabs(sign0 + sign1);
+  const double slope = bounded - q1;
+  return bounded - sign1 * fmax(0.0, fabs(slope) - same * fabs(delta0));
+}
+
+// nonorthogonal_reconstruction.c:61-93 with the interface volume
+// central8(volume) supplied by the caller (it is independent of the
+// variable being reconstructed).  The caller guarantees a finite, nonzero
+// interface volume (checked once at set-up).
+__host__ __device__ inline void up7_pdm(const double vol[8], const double q[8],
+                                        double iv, double pdmb, double *left,
+                                        double *right) {
+  double w[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) w[n] = vol[n] * q[n];
+  const double hl = upwind7_left(w) / iv;
+  const double hr = upwind7_right(w) / iv;
+  *left = pdm_left(q[2], q[3], q[4], hl, pdmb);
+  *right = pdm_left(q[5], q[4], q[3], hr, pdmb);
+}
+
+// nonorthogonal_state.c:60-93
+__host__ __device__ inline int cons_to_prim(const double u[5], double gamma,
+                                            double rho_floor, double p_floor,
+                                            Prim *out) {
+  if (!isfinite(u[0]) || u[0] <= DBL_MIN) return 1;
+  const double raw = u[0];
+  if (!isfinite(u[1]) || !isfinite(u[2]) || !isfinite(u[3])) return 1;
+  const double vx = u[1] / raw;
+  const double vy = u[2] / raw;
+  const double vz = u[3] / raw;
+  double v2 = vx * vx;
+  v2 += vy * vy;
+  v2 += vz * vz;
+  if (!isfinite(u[4])) return 1;
+  const double kinetic = 0.5 * raw * v2;
+  out->vx = vx;
+  out->vy = vy;
+  out->vz = vz;
+  out->rho = fmax(raw, rho_floor);
+  out->p = fmax((gamma - 1.0) * (u[4] - kinetic), p_floor);
+  return 0;
+}
+
+// nonorthogonal_state.c:95-120
+__host__ __device__ inline int prim_to_cons(const Prim &pr, double gamma,
+                                            double rho_floor, double p_floor,
+                                            double u[5]) {
+  if (!isfinite(pr.rho) || !isfinite(pr.p)) return 1;
+  const double rho = fmax(pr.rho, rho_floor);
+  const double p = fmax(pr.p, p_floor);
+  if (!isfinite(pr.vx) || !isfinite(pr.vy) || !isfinite(pr.vz)) return 1;
+  u[0] = rho;
+  u[1] = rho * pr.vx;
+  u[2] = rho * pr.vy;
+  u[3] = rho * pr.vz;
+  double v2 = pr.vx * pr.vx;
+  v2 += pr.vy * pr.vy;
+  v2 += pr.vz * pr.vz;
+  u[4] = p / (gamma - 1.0) + 0.5 * rho * v2;
+  return 0;
+}
+
+// nonorthogonal_state.c:122-159
+__host__ __device__ inline int predict_cell(const double uold[5],
+                                            const double ucur[5], double ratio,
+                                            double gamma, double rho_floor,
+                                            double p_floor, double out[5]) {
+  Prim o, c;
+  if (cons_to_prim(uold, gamma, rho_floor, p_floor, &o) ||
+      cons_to_prim(ucur, gamma, rho_floor, p_floor, &c))
+    return 1;
+  Prim q;
+  q.rho = fmax(c.rho + ratio * (c.rho - o.rho), rho_floor);
+  q.p = fmax(c.p + ratio * (c.p - o.p), p_floor);
+  q.vx = c.vx + ratio * (c.vx - o.vx);
+  q.vy = c.vy + ratio * (c.vy - o.vy);
+  q.vz = c.vz + ratio * (c.vz - o.vz);
+  return prim_to_cons(q, gamma, rho_floor, p_floor, out);
+}
+
+// nonorthogonal_flux.c:25-36
+__host__ __device__ inline bool valid_prim(const Prim &s) {
+  if (!isfinite(s.rho) || !isfinite(s.p) || s.rho <= DBL_MIN ||
+      s.p <= DBL_MIN)
+    return false;
+  return isfinite(s.vx) && isfinite(s.vy) && isfinite(s.vz);
+}
+
+struct FaceFrame {
+  double nx, ny, nz, t1x, t1y, t1z, t2x, t2y, t2z;
+};
+
+struct FluidFlux {
+  double f[5];
+  double jump[5];
+  double vjump[3];
+  double vn[2];
+};
+
+// nonorthogonal_flux.c:38-105
+__device__ inline int kinetic_fluid_flux(const Prim st[2], double gamma,
+                                         const FaceFrame &fr, FluidFlux *fl) {
+  if (!isfinite(gamma) || gamma <= 1.0 || !valid_prim(st[0]) ||
+      !valid_prim(st[1]))
+    return 1;
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    fl->f[m] = 0.0;
+    fl->jump[m] = 0.0;
+  }
+  fl->vjump[0] = fl->vjump[1] = fl->vjump[2] = 0.0;
+  const double pi = 3.14159265358979323846264338327950288;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const double sign = side == 0 ? -1.0 : 1.0;
+    const double rho = st[side].rho;
+    const double p = st[side].p;
+    const double vx = st[side].vx, vy = st[side].vy, vz = st[side].vz;
+    const double v2 = dot3(vx, vy, vz, vx, vy, vz);
+    const double energy = 0.5 * rho * v2 + p / (gamma - 1.0);
+    const double lambda = rho / (2.0 * p);
+    const double vn = dot3(fr.nx, fr.ny, fr.nz, vx, vy, vz);
+    const double vt1 = dot3(fr.t1x, fr.t1y, fr.t1z, vx, vy, vz);
+    const double vt2 = dot3(fr.t2x, fr.t2y, fr.t2z, vx, vy, vz);
+    const double zeroth = 0.5 * erfc(sign * sqrt(lambda) * vn);
+    const double first =
+        vn * zeroth - 0.5 * sign * exp(-lambda * vn * vn) / sqrt(pi * lambda);
+    fl->vn[side] = vn;
+    fl->f[0] += rho * first;
+    fl->f[4] += (energy + 0.5 * p) * first + 0.5 * p * zeroth * vn;
+    const double mn = rho * vn * first + p * zeroth;
+    const double mt1 = rho * vt1 * first;
+    const double mt2 = rho * vt2 * first;
+    fl->f[1] += fr.nx * mn + fr.t1x * mt1 + fr.t2x * mt2;
+    fl->vjump[0] += sign * vx;
+    fl->f[2] += fr.ny * mn + fr.t1y * mt1 + fr.t2y * mt2;
+    fl->vjump[1] += sign * vy;
+    fl->f[3] += fr.nz * mn + fr.t1z * mt1 + fr.t2z * mt2;
+    fl->vjump[2] += sign * vz;
+    fl->jump[0] += sign * rho;
+    fl->jump[1] += sign * rho * vx;
+    fl->jump[2] += sign * rho * vy;
+    fl->jump[3] += sign * rho * vz;
+    fl->jump[4] += sign * energy;
+  }
+  return 0;
+}
+
+struct MaxwellFlux {
+  double m[3];
+  double alfven;
+  double pmag;
+};
+
+// nonorthogonal_flux.c:107-173
+__device__ inline int kinetic_maxwell_flux(
+    const Prim st[2], const double b[2][3], double bn, const FaceFrame &fr,
+    bool use_bg, const double b0[3], double b0n, bool use_boris, double c,
+    const double vn[2], MaxwellFlux *mx) {
+  if (!isfinite(bn) || (use_boris && (!isfinite(c) || c <= DBL_MIN))) return 1;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    if (!valid_prim(st[side])) return 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (!isfinite(b[side][d]) || (use_bg && !isfinite(b0[d]))) return 1;
+  }
+  mx->m[0] = mx->m[1] = mx->m[2] = 0.0;
+  mx->alfven = 0.0;
+  mx->pmag = 0.0;
+  const double nrm[3] = {fr.nx, fr.ny, fr.nz};
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const double sign = side == 0 ? -1.0 : 1.0;
+    const double r2 = dot3(b[side][0], b[side][1], b[side][2], b[side][0],
+                           b[side][1], b[side][2]);
+    const double rp = 0.5 * r2;
+    double tx = b[side][0], ty = b[side][1], tz = b[side][2];
+    if (use_bg) {
+      tx = b[side][0] + b0[0];
+      ty = b[side][1] + b0[1];
+      tz = b[side][2] + b0[2];
+    }
+    const double t2 = dot3(tx, ty, tz, tx, ty, tz);
+    const double va2 = t2 / st[side].rho;
+    const double cva2 = use_boris ? va2 / (1.0 + va2 / (c * c)) : va2;
+    const double lambda = 1.0 / (2.0 * st[side].p / st[side].rho + cva2);
+    const double zeroth = 0.5 * erfc(sign * sqrt(lambda) * vn[side]);
+    mx->alfven += 0.5 * sqrt(cva2);
+    mx->pmag += 0.5 * t2;
+    const double bdr =
+        use_bg ? dot3(b0[0], b0[1], b0[2], b[side][0], b[side][1], b[side][2])
+               : 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double stress = rp * nrm[d] - b[side][d] * bn;
+      if (use_bg)
+        stress += -b0[d] * bn - b[side][d] * b0n + bdr * nrm[d];
+      mx->m[d] += zeroth * stress;
+    }
+  }
+  return 0;
+}
+
+// nonorthogonal_flux.c:175-204 (options were validated at entry)
+__device__ inline void apply_hogs(FluidFlux *fl, MaxwellFlux *mx, double ch,
+                                  double cm, bool use_boris, double c) {
+#pragma unroll
+  for (int m = 0; m < 5; ++m) fl->f[m] -= ch * mx->alfven * fl->jump[m];
+  if (use_boris) {
+    const double ic2 = 1.0 / (c * c);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double j = mx->pmag * fl->vjump[d] * ic2;
+      mx->m[d] -= cm * mx->alfven * j;
+    }
+  }
+}
+
+// nonorthogonal_flux.c:206-241 (use_boris is true at every call site)
+__device__ inline int emergency_diffusion(FluidFlux *fl, const Prim st[2],
+                                          const double lo[5],
+                                          const double hi[5], double c,
+                                          bool *applied, double *speed) {
+  *applied = false;
+  double s2 = 0.0;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    if (!valid_prim(st[side])) return 1;
+    s2 += dot3(st[side].vx, st[side].vy, st[side].vz, st[side].vx,
+               st[side].vy, st[side].vz);
+  }
+  const double is = sqrt(0.5 * s2);
+  *speed = is;
+  if (is < 1.5 * c) return 0;
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    if (!isfinite(lo[m]) || !isfinite(hi[m])) return 1;
+    fl->f[m] -= c * (hi[m] - lo[m]);
+  }
+  *applied = true;
+  return 0;
+}
+
+// nonorthogonal_operators.c:144-182 (length > DBL_MIN checked at set-up)
+__device__ inline int edge_emf(double vt1, double vt2, double bt1, double bt2,
+                               double jump, double rho, double length,
+                               double diffusion, bool use_boris, double c,
+                               double cfl, double dt, double *emf) {
+  if (!isfinite(vt1) || !isfinite(vt2) || !isfinite(bt1) || !isfinite(bt2) ||
+      !isfinite(jump) || !isfinite(rho) || rho <= DBL_MIN)
+    return 1;
+  const double flow = hypot(vt1, vt2);
+  double va = hypot(bt1, bt2) / sqrt(rho);
+  if (use_boris) va = c * va / hypot(c, va);
+  double speed = flow + va;
+  speed = fmin(speed, cfl * length / dt);
+  const double ideal = -(vt1 * bt2 - vt2 * bt1);
+  *emf = (ideal + diffusion * speed * jump) * length;
+  return 0;
+}
+
+// nonorthogonal_state.c:161-174 (+ vector helpers :9-52)
+__device__ inline int apply_boris(double u[5], const double uold[5],
+                                  const double bnew[3], const double bold[3],
+                                  const double rate[5], const double mrate[3],
+                                  double c, double dt, double gamma,
+                                  double rho_floor, double p_floor) {
+  Prim up;
+  if (cons_to_prim(u, gamma, rho_floor, p_floor, &up) || uold[0] <= DBL_MIN)
+    return 1;
+  const double urho = fmax(up.rho, rho_floor);
+  const double up_p = fmax(up.p, p_floor);
+  const double orho = uold[0];
+  double ov[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ov[d] = uold[1 + d] / fmax(orho, rho_floor);
+  double half[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) half[d] = 0.5 * (bnew[d] + bold[d]);
+  const double alpha = dot3(half[0], half[1], half[2], half[0], half[1],
+                            half[2]) /
+                       (urho * c * c);
+  const double drho = dt * rate[0];
+  double gas[3], mag[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    gas[d] = dt * rate[1 + d];
+    mag[d] = dt * mrate[d];
+  }
+  double inc[3];
+  if (alpha > 1.0e-12) {
+    const double frac = 1.0 / (1.0 + alpha);
+    // normalized_or_zero (nonorthogonal_state.c:45-52)
+    const double norm =
+        sqrt(dot3(half[0], half[1], half[2], half[0], half[1], half[2]));
+    double unit[3] = {0.0, 0.0, 0.0};
+    if (!(norm <= 1.0e-12)) {
+      const double inv = 1.0 / norm;
+      unit[0] = inv * half[0];
+      unit[1] = inv * half[1];
+      unit[2] = inv * half[2];
+    }
+    double tot[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) tot[d] = gas[d] + mag[d];
+    // vector_parallel(gas, unit) = unit * dot(gas, unit)
+    const double gp = dot3(gas[0], gas[1], gas[2], unit[0], unit[1], unit[2]);
+    const double tp = dot3(tot[0], tot[1], tot[2], unit[0], unit[1], unit[2]);
+    const double vp = dot3(ov[0], ov[1], ov[2], unit[0], unit[1], unit[2]);
+    const double k = alpha * frac * drho;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double par = gp * unit[d];
+      const double tperp = tot[d] - tp * unit[d];
+      const double vperp = ov[d] - vp * unit[d];
+      inc[d] = par + (frac * tperp + k * vperp);
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) inc[d] = gas[d] + mag[d];
+  }
+  Prim res;
+  res.rho = urho;
+  res.p = up_p;
+  res.vx = (orho * ov[0] + inc[0]) / urho;
+  res.vy = (orho * ov[1] + inc[1]) / urho;
+  res.vz = (orho * ov[2] + inc[2]) / urho;
+  return prim_to_cons(res, gamma, rho_floor, p_floor, u);
+}
+
+// nonorthogonal_state.c:109-143 (apply_maxwell)
+__device__ inline int apply_maxwell(double u[5], const double mrate[3],
+                                    double dt, double gamma, double rho_floor,
+                                    double p_floor) {
+  const double rho = fmax(u[0], rho_floor);
+  double m2 = u[1] * u[1];
+  m2 += u[2] * u[2];
+  m2 += u[3] * u[3];
+  const double p = fmax((gamma - 1.0) * (u[4] - 0.5 * m2 / rho), p_floor);
+  u[1] += dt * mrate[0];
+  u[2] += dt * mrate[1];
+  u[3] += dt * mrate[2];
+  double n2 = u[1] * u[1];
+  n2 += u[2] * u[2];
+  n2 += u[3] * u[3];
+  u[0] = rho;
+  u[4] = 0.5 * n2 / rho + p / (gamma - 1.0);
+  return 0;
+}
+
+}  // namespace gcs

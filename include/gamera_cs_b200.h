@@ -1,0 +1,187 @@
+/*
+ * libgamera_cs_b200 — B200 (sm_100a) implementation of the GAMERA-Cube
+ * six-face cubed-sphere MHD step and ionosphere potential solve.
+ *
+ * Part 1 declares drop-in replacements for the reference C entry points:
+ * same names, signatures, argument meaning and return convention (0 ok,
+ * -1 error; state may be partially updated on error).  Each cites the
+ * reference declaration it replaces.  All six faces are kept resident on
+ * the current CUDA device; host arrays in the reference layout are uploaded
+ * before and downloaded after every call unless a context is put into
+ * resident mode (Part 2).
+ *
+ * Part 2 is the device-resident context API used by callers that keep the
+ * state on the GPU between steps (benchmarks, multi-step drivers).  It has
+ * no counterpart in the reference.
+ */
+#ifndef GAMERA_CS_B200_H
+#define GAMERA_CS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "gamera_cs_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- Part 1 */
+
+/* cubedsphere/cubedsphere_halo.h:12.  Here the plan also owns the device
+ * copy of the grid, its derived constants and the device state. */
+typedef struct gamera_cs_halo_plan gamera_cs_halo_plan;
+
+/* cubedsphere/cubedsphere_step.h:16-21 */
+int gamera_cs_advance_six(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                          gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                          const size_t active[3], size_t ghost,
+                          double predictor_ratio, double dt,
+                          const gamera_no_advance_options *options);
+
+/* cubedsphere/cubedsphere_step.h:33-40 */
+int gamera_cs_advance_six_with_boundary(
+    const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT], const size_t active[3],
+    size_t ghost, double predictor_ratio, double dt,
+    const gamera_no_advance_options *options,
+    gamera_cs_radial_boundary_function radial_boundary, double current_time,
+    double previous_time, void *boundary_context);
+
+/* cubedsphere/cubedsphere_step.h:46-54 */
+int gamera_cs_advance_six_with_background(
+    const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT], const size_t active[3],
+    size_t ghost, double predictor_ratio, double dt,
+    const gamera_no_advance_options *options,
+    const gamera_no_background_field background[GAMERA_CS_FACE_COUNT],
+    gamera_cs_radial_boundary_function radial_boundary, double current_time,
+    double previous_time, void *boundary_context);
+
+/* cubedsphere/cubedsphere_step.h:58-67 */
+int gamera_cs_advance_six_with_background_planned(
+    const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT], const size_t active[3],
+    size_t ghost, double predictor_ratio, double dt,
+    const gamera_no_advance_options *options,
+    const gamera_no_background_field background[GAMERA_CS_FACE_COUNT],
+    const gamera_cs_halo_plan *halo_plan,
+    gamera_cs_radial_boundary_function radial_boundary, double current_time,
+    double previous_time, void *boundary_context);
+
+/* cubedsphere/cubedsphere_halo.h:37-40 */
+int gamera_cs_halo_plan_create(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                               const size_t active[3], size_t ghost,
+                               gamera_cs_halo_plan **out);
+void gamera_cs_halo_plan_destroy(gamera_cs_halo_plan *plan);
+
+/* cubedsphere/cubedsphere_halo.h:46-53 */
+int gamera_cs_fill_tangential_cell_halos_planned(
+    const gamera_cs_halo_plan *plan,
+    const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT]);
+int gamera_cs_fill_magnetic_face_halos_planned(
+    const gamera_cs_halo_plan *plan,
+    const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT]);
+
+/* cubedsphere/cubedsphere_halo.h:32 */
+int gamera_cs_halo_valid_state(const double state[GAMERA_NO_FLUX_COUNT]);
+
+/* ---------------------------------------------------------------- Part 2 */
+
+typedef struct gcs_context gcs_context;
+
+/* Stage codes reported by gcs_context_failure (first failing stage). */
+enum {
+  GCS_STAGE_NONE = 0,
+  GCS_STAGE_PREDICT = 1,
+  GCS_STAGE_RECOVER_PREDICT = 2,
+  GCS_STAGE_RECONSTRUCT = 3,
+  GCS_STAGE_KINETIC_FLUID = 4,
+  GCS_STAGE_KINETIC_MAXWELL = 5,
+  GCS_STAGE_EMERGENCY = 6,
+  GCS_STAGE_EDGE_GEOMETRY = 7,
+  GCS_STAGE_EDGE_VELOCITY = 8,
+  GCS_STAGE_TRANSVERSE = 9,
+  GCS_STAGE_EDGE_DENSITY = 10,
+  GCS_STAGE_EDGE_EMF = 11,
+  GCS_STAGE_UPDATE = 12,
+  GCS_STAGE_RECOVER_UPDATE = 13,
+  GCS_STAGE_RECOVER_FINAL = 14,
+  GCS_STAGE_TIMESTEP = 15,
+  GCS_STAGE_HOST = 16,
+  GCS_STAGE_SOLVE_EDGE = 17,
+  GCS_STAGE_OPTIONS = 18
+};
+
+/* Build a device context from a host grid in the reference layout
+ * (all six faces; active[1] == active[2] >= 9; ghost == 4).  Returns NULL on
+ * failure; gcs_last_error() then describes it. */
+gcs_context *gcs_context_create(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                const size_t active[3], size_t ghost);
+void gcs_context_destroy(gcs_context *ctx);
+const char *gcs_last_error(void);
+const char *gcs_context_error(const gcs_context *ctx);
+
+int gcs_context_upload_background(
+    gcs_context *ctx,
+    const gamera_no_background_field background[GAMERA_CS_FACE_COUNT]);
+int gcs_context_upload_state(gcs_context *ctx,
+                             const gamera_no_storage storage[GAMERA_CS_FACE_COUNT]);
+/* include_scratch != 0 also downloads predicted arrays, fluid/Maxwell face
+ * fluxes and edge EMFs of the last step. */
+int gcs_context_download_state(gcs_context *ctx,
+                               gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                               int include_scratch);
+
+/* One step on the device-resident state (no host transfers); same stage
+ * order and options as gamera_cs_advance_six_with_background_planned with
+ * outflow radial ghosts and no callbacks. */
+int gcs_context_step(gcs_context *ctx, const gamera_no_advance_options *options,
+                     double predictor_ratio, double dt);
+
+/* Minimum CFL step over the active cells of all faces
+ * (nonorthogonal_step.c:449-525, reduced over the six faces). */
+int gcs_context_timestep(gcs_context *ctx,
+                         const gamera_no_timestep_options *options,
+                         double *dt);
+
+/* Driver loop on the device: before the first call the step size is
+ * dt_fraction * timestep; each step then sets
+ * dt = min(dt_fraction * cfl_min, 1.25 dt_prev) and the predictor ratio
+ * 0.5 dt / dt_prev on the device.  use_graph != 0 replays one captured
+ * CUDA graph per step.  Does not synchronise; call gcs_context_sync. */
+int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
+                    const gamera_no_timestep_options *timestep,
+                    double dt_fraction, int steps, int use_graph);
+int gcs_context_sync(gcs_context *ctx);
+int gcs_context_params(gcs_context *ctx, double *dt, double *ratio,
+                       double *cfl_min, int *steps);
+int gcs_context_set_params(gcs_context *ctx, double dt, double ratio,
+                           double dt_prev, int steps);
+/* First failure since the last reset; returns the stage code (0 = none). */
+int gcs_context_failure(gcs_context *ctx, int *dir, int *face, int *i, int *j,
+                        int *k);
+int gcs_context_reset_failure(gcs_context *ctx);
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
+uintptr_t gcs_context_stream(gcs_context *ctx);
+/* Profiling: record CUDA events around each stage of every step. */
+int gcs_context_set_profiling(gcs_context *ctx, int on);
+/* Accumulated device milliseconds and launch counts per stage since
+ * profiling was switched on; returns the number of stages written. */
+int gcs_context_stage_times(gcs_context *ctx, double *ms, long long *calls,
+                            int capacity);
+const char *gcs_stage_name(int stage_slot);
+size_t gcs_context_device_bytes(const gcs_context *ctx);
+/* Resident mode: the device copy stays authoritative between drop-in calls
+ * made with the same storage pointer; gcs_context_download_state copies it
+ * back explicitly. */
+gcs_context *gcs_halo_plan_context(gamera_cs_halo_plan *plan);
+int gcs_context_set_resident(gcs_context *ctx, int on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -29,12 +29,15 @@
 #include "nonorthogonal_state.h"
 #include "nonorthogonal_step.h"
 
+#include "cases_common.h"
+
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
-enum { FX_UNIFORM = 0, FX_SHOCK = 1, FX_WIND = 2, FX_PULSE = 3 };
+enum { FX_UNIFORM = CASE_UNIFORM, FX_SHOCK = CASE_SHOCK, FX_WIND = CASE_WIND,
+       FX_PULSE = CASE_PULSE };
 
 typedef struct {
   int kind;
@@ -57,27 +60,10 @@ typedef struct {
   unsigned long long seed;
 } fx_case;
 
-/* Code units of the reference Earth driver: x in R_E, u in 100 km/s,
- * rho in proton cm^-3 (test_cubedsphere_dipole_background.c:467-471). */
-static const double fx_rho_norm = 1.67262192369e-21;
-static const double fx_dipole_moment = -6761.730688424097;
+double fx_magnetic_norm_tesla(void) { return case_magnetic_norm_tesla(); }
 
-double fx_magnetic_norm_tesla(void) {
-  return 100000.0 * sqrt(4.0e-7 * acos(-1.0) * fx_rho_norm);
-}
-
-static uint64_t splitmix64(uint64_t x) {
-  x += 0x9e3779b97f4a7c15ULL;
-  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
-  x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
-  return x ^ (x >> 31);
-}
-
-/* Uniform in [-1, 1), from the seed, face and storage cell index only. */
 double fx_noise(unsigned long long seed, int face, size_t cell) {
-  const uint64_t h = splitmix64(splitmix64((uint64_t)seed) ^
-                                ((uint64_t)face << 56) ^ (uint64_t)cell);
-  return 2.0 * ((double)(h >> 11) * 0x1.0p-53) - 1.0;
+  return case_noise(seed, face, cell);
 }
 
 static int uniform_potential(gamera_no_vec3 point, void *context,
@@ -146,15 +132,14 @@ fx_case *fx_create(int kind, size_t nr, size_t n, unsigned long long seed) {
     free(c);
     return NULL;
   }
-  gamera_no_dipole dipole = {{{0.0, 0.0, fx_dipole_moment}}};
+  gamera_no_dipole dipole = {{{0.0, 0.0, CASE_DIPOLE_MOMENT}}};
   c->use_background = wind;
   const double bnorm = fx_magnetic_norm_tesla();
   if (wind) {
     c->wind_density = 5.0;
     c->wind_speed = kind == FX_PULSE ? -4.5 : -4.0;
     /* n k T / (rho_norm u_norm^2), protons only, T = 1e5 K. */
-    c->wind_pressure = 5.0e6 * 1.380649e-23 * 1.0e5 /
-                       (fx_rho_norm * 1.0e10);
+    c->wind_pressure = case_wind_pressure();
     c->imf = (gamera_no_vec3){{0.0, 0.0, -5.0e-9 / bnorm}};
     c->pulse_amplitude = kind == FX_PULSE ? 0.2 : 0.0;
     c->pulse_wavelength = 10.0;
@@ -200,11 +185,7 @@ fx_case *fx_create(int kind, size_t nr, size_t n, unsigned long long seed) {
                     : (gamera_no_primitive){0.125, {{0.0, 0.0, 0.0}}, 0.1};
       } else {
         const gamera_no_vec3 x = c->grid[f].cell[cell].centroid;
-        double rho = c->wind_density * (1.0 + 0.01 * fx_noise(seed, f, cell));
-        if (c->pulse_amplitude != 0.0)
-          rho *= 1.0 + c->pulse_amplitude *
-                           sin(2.0 * acos(-1.0) * x.value[0] /
-                               c->pulse_wavelength);
+        const double rho = case_wind_density(kind, seed, f, cell, x.value[0]);
         p = (gamera_no_primitive){rho, {{c->wind_speed, 0.0, 0.0}},
                                   c->wind_pressure};
       }

@@ -1,0 +1,379 @@
+"""Benchmark: six-face cubed-sphere MHD step on B200 (plain FP64 path).
+
+Workload (the production-size configuration): each cube face 96 x 96
+angular x 192 radial active cells (10,616,832 cells), 4 ghost layers,
+log-stretched r in [2.5, 30] R_E, uniform solar wind n = 5 cm^-3,
+V = -400 km/s, T = 1e5 K, IMF Bz = -5 nT, aligned 3.1e-5 T Earth dipole
+background, seeded +-1 % density noise, CFL 0.3 with the reference Earth
+driver's dt rule; outflow radial ghosts.  Synthetic state built on the
+device; state arrays are several GB, far larger than L2.
+
+Metric: cell-updates/s (active cells x steps / device time), whole job
+over all ranks.  --gpus N runs N independent replicas (one per GPU, weak
+scaling: the step has no inter-GPU exchange).
+
+--impl reference times the reference's own CPU step (oracle/_ref, the
+unmodified reference library, all host threads) on a bounded sample of the
+same workload.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+NR, N = 192, 96                 # active radial, angular cells per face
+KIND_WIND = 2
+METRIC = "MHD cell-updates/s on 1 B200 (FP64 plain path)"
+# Algorithmic bytes per cell-update of the whole step (state 192 B +
+# compacted metric 664 B + background 192 B).
+STEP_BYTES_PER_CELL = 1048
+# Per-launch algorithmic bytes per face of the flux sweep: cells U~ (5),
+# B~ (3), volume (1) counted once per face along the sweep, face Phi~ (1),
+# area (1), frame (9), central8 volume (1), B0 face (3) + B0 normal (1),
+# written fluid (5) + Maxwell (3) flux: 33 doubles.
+FLUX_BYTES_PER_FACE = 33 * 8
+# Edge EMF per edge: face velocities (3) and areas (1) of one face family,
+# Phi~ (2) and areas (1) of the other, edge frame (6), 2x2 system (5),
+# central8 area sums (2), length (1), B0 projections (2), edge density
+# cells (1), written EMF (1): 25 doubles (each counted once per edge).
+EMF_BYTES_PER_EDGE = 25 * 8
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.file.flush()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.file.name) as fh:
+                for line in fh:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 7:
+                        rows.append(parts)
+        finally:
+            os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[0]) for r in rows if r[0].replace(".", "").isdigit())
+        mx = max(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4)
+                          if r[3 + q].lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init(n_gpus):
+    if n_gpus <= 1 or "RANK" not in os.environ:
+        return 0, 1, None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist.get_rank(), dist.get_world_size(), dist
+
+
+def max_over_ranks(value, dist, device):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value, dist, device):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist, device):
+    if dist is not None:
+        import torch
+        dist.barrier(device_ids=[device.index])
+        torch.cuda.synchronize(device)
+
+
+def run_gpu(args):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    rank, world, dist = dist_init(args.gpus)
+    import gamera_cube_b200
+    from gamera_cube_b200 import abi
+    from gamera_cube_b200.host import HostStorage
+    lib = gamera_cube_b200.lib
+    nr, n = args.nr, args.n
+    cells = 6 * nr * n * n
+
+    t0 = time.time()
+    ctx = lib.gcs_context_create_case(KIND_WIND, nr, n, 1000 + rank)
+    if not ctx:
+        raise RuntimeError(lib.gcs_last_error().decode())
+    setup_s = time.time() - t0
+    opts, ts = abi.AdvanceOptions(), abi.TimestepOptions()
+    lib.gcs_case_options(KIND_WIND, C.byref(opts), C.byref(ts))
+    stream = torch.cuda.ExternalStream(lib.gcs_context_stream(ctx), device=device)
+
+    # warm-up (also captures the CUDA graph of one step)
+    if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, args.warmup, 1):
+        raise RuntimeError("warm-up failed")
+    if lib.gcs_context_sync(ctx) != 0:
+        raise RuntimeError("warm-up step failed")
+
+    # ---- timed region: K graph-replayed steps, device time on the stream
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(
+        enable_timing=True)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, args.steps, 1):
+            raise RuntimeError("timed run failed")
+        stop.record(stream)
+        torch.cuda.synchronize(device)
+    barrier(dist, device)
+    if lib.gcs_context_sync(ctx) != 0:
+        raise RuntimeError("a timed step failed")
+    ms_local = start.elapsed_time(stop)
+    ms = max_over_ranks(ms_local, dist, device)
+    total_cells = sum_over_ranks(float(cells), dist, device)
+    value = total_cells * args.steps / (ms * 1e-3)
+
+    # ---- per-stage device times (CUDA events around each stage, same
+    # stream, no graph) for the roofline of the dominant kernel
+    lib.gcs_context_set_profiling(ctx, 1)
+    prof_steps = max(2, min(args.steps, 5))
+    barrier(dist, device)
+    if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, prof_steps, 0):
+        raise RuntimeError("profiled run failed")
+    stage_ms = (C.c_double * 16)()
+    stage_calls = (C.c_longlong * 16)()
+    nst = lib.gcs_context_stage_times(ctx, stage_ms, stage_calls, 16)
+    lib.gcs_context_set_profiling(ctx, 0)
+    stages = {lib.gcs_stage_name(q).decode(): stage_ms[q] / prof_steps
+              for q in range(nst)}
+    step_ms_prof = sum(stages.values())
+    dom = max(stages, key=stages.get)
+    faces_per_dir = 6 * (nr * n * n + n * n)          # ~ faces of one family
+    edges_per_dir = 6 * (nr * (n + 1) * (n + 1))
+    if dom == "flux":
+        alg = 3 * faces_per_dir * FLUX_BYTES_PER_FACE
+    elif dom == "edge_emf":
+        alg = 3 * edges_per_dir * EMF_BYTES_PER_EDGE
+    else:
+        alg = cells * STEP_BYTES_PER_CELL
+    per_launch_ms = stages[dom] / 3.0 if dom in ("flux", "edge_emf") else stages[dom]
+    hbm, peak_kind = peaks()
+    achieved = (alg / 3.0 if dom in ("flux", "edge_emf") else alg) / (
+        per_launch_ms * 1e-3) / 1e9
+
+    # ---- end to end through the drop-in step with pinned host buffers
+    act = (C.c_size_t * 3)()
+    g = C.c_size_t()
+    lib.gcs_context_dims(ctx, act, C.byref(g))
+    hs = HostStorage(list(act), g.value, pinned=True, scratch=False)
+    if lib.gcs_context_download_state(ctx, hs.storage, 0) != 0:
+        raise RuntimeError("download failed")
+    dtv, ratio = C.c_double(), C.c_double()
+    lib.gcs_context_params(ctx, C.byref(dtv), C.byref(ratio), None, None)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        if lib.gcs_context_advance_host(ctx, hs.storage, C.byref(opts), 0.5,
+                                        dtv.value) != 0:
+            raise RuntimeError("drop-in step failed")
+    torch.cuda.synchronize(device)
+    e2e_s = max_over_ranks(time.perf_counter() - t1, dist, device)
+    barrier(dist, device)
+    e2e_value = total_cells * e2e_steps / e2e_s
+
+    result = None
+    if rank == 0:
+        clk = clocks.summary()
+        launches_per_step = 24
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "cell-updates/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded solar wind + dipole, built on the device)",
+            "config": {"workload": "cubed-sphere 6 x %dx%dx%d FP64 MHD step, "
+                                   "solar wind + aligned dipole" % (n, n, nr),
+                       "faces": 6, "angular": n, "radial": nr,
+                       "cells_per_gpu": cells, "ghost": 4,
+                       "graph": "one CUDA graph per step, device-side dt",
+                       "l2": "state arrays larger than L2 (no flush needed)",
+                       "parallelism": "replicas x%d" % world,
+                       "setup_s": round(setup_s, 2)},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": hs.bytes_state,
+                    "d2h_bytes_per_step": hs.bytes_state,
+                    "call": "gcs_context_advance_host (drop-in step, pinned host "
+                            "buffers, %d steps)" % e2e_steps},
+            "roofline": {"bound": "hbm", "kernel": dom,
+                         "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6650 GB/s",
+                         "traffic": None,
+                         "step_share": stages[dom] / step_ms_prof,
+                         "step_hbm_frac": cells * STEP_BYTES_PER_CELL /
+                         (ms_local / args.steps * 1e-3) / 1e9 / hbm},
+            "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        }
+        if args.cpu_baseline and world == 1:
+            result["cpu_baseline"] = cpu_baseline(args)
+    lib.gcs_context_destroy(ctx)
+    if dist is not None:
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result))
+
+
+def _ref_bench_path():
+    return os.path.join(REPO, "oracle", "_ref", "ref_bench")
+
+
+def cpu_baseline(args, steps=None):
+    """The reference's own CPU step on a bounded sample of the workload (the
+    same case at 48 radial x 16 x 16 angular cells per face), all host
+    threads; falls back to the CPU restatement (one thread) if the
+    reference library was not built."""
+    nr, n = args.cpu_nr, args.cpu_n
+    steps = steps or args.cpu_steps
+    exe = _ref_bench_path()
+    threads = os.cpu_count() or 1
+    if os.path.exists(exe):
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close",
+                   OMP_PLACES="cores")
+        out = subprocess.run([exe, "2", str(nr), str(n), "1", str(steps), "1000"],
+                             capture_output=True, text=True, env=env, timeout=900)
+        if out.returncode != 0:
+            raise RuntimeError("reference CPU run failed: " + out.stderr[-500:])
+        rec = json.loads(out.stdout.strip().splitlines()[-1])
+        return {"value": rec["cell_updates_per_s"], "unit": "cell-updates/s",
+                "cores": rec["threads"], "kind": "reference",
+                "sample": "reference CPU step (OpenMP), 6 x %dx%dx%d wind+dipole "
+                          "case, %d timed steps after 1 warm-up" % (n, n, nr, steps)}
+    from oracle import oracle_cases
+    case = oracle_cases.Case("wind", nr, n, 1000)
+    dt = 0.5 * case.local_timestep()
+    case.step(0.0, dt)
+    t = time.perf_counter()
+    for _ in range(steps):
+        case.step(0.5, dt)
+    sec = time.perf_counter() - t
+    return {"value": 6 * nr * n * n * steps / sec, "unit": "cell-updates/s",
+            "cores": 1, "kind": "port",
+            "sample": "CPU restatement, 6 x %dx%dx%d wind+dipole case, %d steps"
+                      % (n, n, nr, steps)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    base = cpu_baseline(args, steps=min(steps, args.cpu_steps))
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"],
+            "unit": base["unit"], "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cubed-sphere 6 x %dx%dx%d FP64 MHD step, "
+                                   "solar wind + aligned dipole (bounded CPU "
+                                   "sample 6 x %dx%dx%d)" % (
+                                       args.n, args.n, args.nr, args.cpu_n,
+                                       args.cpu_n, args.cpu_nr)},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": base["unit"],
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nr", type=int, default=NR)
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--cpu-nr", type=int, default=48)
+    ap.add_argument("--cpu-n", type=int, default=16)
+    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

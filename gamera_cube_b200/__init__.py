@@ -69,6 +69,18 @@ def _load():
         "gcs_context_device_bytes": (C.c_size_t, [C.c_void_p]),
         "gcs_halo_plan_context": (C.c_void_p, [C.c_void_p]),
         "gcs_context_set_resident": (C.c_int, [C.c_void_p, C.c_int]),
+        "gcs_context_create_case": (C.c_void_p, [C.c_int, C.c_size_t, C.c_size_t,
+                                                 C.c_ulonglong]),
+        "gcs_case_options": (C.c_int, [C.c_int, P(abi.AdvanceOptions),
+                                       P(abi.TimestepOptions)]),
+        "gcs_context_dims": (C.c_int, [C.c_void_p, P(C.c_size_t),
+                                       P(C.c_size_t)]),
+        "gcs_context_advance_host": (C.c_int, [C.c_void_p, P(abi.Storage),
+                                               P(abi.AdvanceOptions), C.c_double,
+                                               C.c_double]),
+        "gcs_context_debug_array": (C.c_int, [C.c_void_p, C.c_int, C.c_int,
+                                              C.c_int, C.c_int, P(C.c_double),
+                                              C.c_size_t]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -340,20 +340,25 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
                  const gamera_no_background_field background[6],
                  gamera_cs_radial_boundary_function radial, double t,
                  double tprev, void *radial_ctx) {
-  if (ctx == nullptr || grid == nullptr || storage == nullptr ||
-      active == nullptr || options == nullptr || ghost < 4 ||
-      !std::isfinite(dt) || dt <= 0.0 ||
+  // grid == nullptr: a context built on the device (gcs_context_create_case)
+  // with its own background; host callbacks are then not available.
+  if (ctx == nullptr || storage == nullptr || active == nullptr ||
+      options == nullptr || ghost < 4 || !std::isfinite(dt) || dt <= 0.0 ||
       (radial != nullptr && (!std::isfinite(t) || !std::isfinite(tprev))) ||
       !std::isfinite(ratio) || active[1] != active[2])
     return -1;
   gcs::Context &C = ctx->c;
-  if (!C.grid_matches(grid) || (size_t)C.X.D.nr != active[0] ||
-      (size_t)C.X.D.n != active[1] || (size_t)C.X.D.g != ghost)
+  if ((grid != nullptr && !C.grid_matches(grid)) ||
+      (grid == nullptr && (radial || options->fluid_flux_sync ||
+                           options->edge_emf_sync)) ||
+      (size_t)C.X.D.nr != active[0] || (size_t)C.X.D.n != active[1] ||
+      (size_t)C.X.D.g != ghost)
     return -1;
   gcs::Opts O;
-  if (!make_opts(options, background != nullptr, &O)) return -1;
+  const bool own_bg = grid == nullptr && C.bg_uploaded;
+  if (!make_opts(options, background != nullptr || own_bg, &O)) return -1;
   if (O.u_mhd && !(std::isfinite(dt) && dt > DBL_MIN)) return -1;
-  if (O.u_bg) {
+  if (O.u_bg && !own_bg) {
     for (int f = 0; f < 6; ++f)
       for (int d = 0; d < 3; ++d)
         if (background[f].face_magnetic[d] == nullptr ||
@@ -510,6 +515,107 @@ int gamera_cs_halo_valid_state(const double state[5]) {
 gcs_context *gcs_context_create(const gamera_no_grid grid[6],
                                 const size_t active[3], size_t ghost) {
   return create_context(grid, active, ghost);
+}
+
+gcs_context *gcs_context_create_case(int kind, size_t nr, size_t n,
+                                     unsigned long long seed) {
+  gcs_context *ctx = new (std::nothrow) gcs_context;
+  if (!ctx) {
+    set_last("out of host memory");
+    return nullptr;
+  }
+  if (ctx->c.init_case(kind, nr, n, seed) != 0) {
+    set_last(ctx->c.error);
+    delete ctx;
+    return nullptr;
+  }
+  return ctx;
+}
+
+int gcs_case_options(int kind, gamera_no_advance_options *o,
+                     gamera_no_timestep_options *t) {
+  if (!o || !t || kind < 0 || kind > 3) return -1;
+  const double g = 5.0 / 3.0;
+  std::memset(o, 0, sizeof(*o));
+  std::memset(t, 0, sizeof(*t));
+  if (kind == 0) {
+    o->stress = {g, 1e-12, 1e-12, 1.0, 0.0, 0.0, 100.0, true, false, false, false};
+    o->emf = {1e-12, 1.0, 0.0, 100.0, 0.8, 0.01, false, false};
+    o->update = {g, 1e-12, 1e-12, 100.0, true, false, false};
+    *t = {g, 1e-12, 1e-12, 0.8, 100.0, true, false, false};
+  } else if (kind == 1) {
+    o->stress = {g, 1e-12, 1e-12, 1.0, 0.25, 0.25, 100.0, true, true, false, false};
+    o->emf = {1e-12, 1.0, 0.5, 100.0, 0.3, 0.001, false, false};
+    o->update = {g, 1e-12, 1e-12, 100.0, true, false, false};
+    *t = {g, 1e-12, 1e-12, 0.3, 100.0, true, false, false};
+  } else {
+    // Earth driver options (test_cubedsphere_dipole_background.c:405-444)
+    o->stress = {g, 1e-6, 1e-8, 1.0, 0.25, 0.25, 10.0, true, true, true, true};
+    o->emf = {1e-6, 1.0, 0.5, 10.0, 0.3, 0.0, true, true};
+    o->update = {g, 1e-6, 1e-8, 10.0, true, true, true};
+    *t = {g, 1e-6, 1e-8, 0.3, 10.0, true, true, true};
+  }
+  return 0;
+}
+
+int gcs_context_advance_host(gcs_context *ctx, gamera_no_storage storage[6],
+                             const gamera_no_advance_options *options,
+                             double predictor_ratio, double dt) {
+  if (!ctx) return -1;
+  const size_t active[3] = {(size_t)ctx->c.X.D.nr, (size_t)ctx->c.X.D.n,
+                            (size_t)ctx->c.X.D.n};
+  return drop_in_step(ctx, nullptr, storage, active, (size_t)ctx->c.X.D.g,
+                      predictor_ratio, dt, options, nullptr, nullptr, 0.0, 0.0,
+                      nullptr);
+}
+
+// Copy one device node array (nodes_per_face doubles of face `face`) to the
+// host, for diagnostics and set-up tests.  which: 0 volume, 1 area[d],
+// 2 face normal[d][q], 3 face t1[d][q], 4 face t2[d][q], 5 B0 cell[q],
+// 6 B0 force[q], 7 face B0[d][q], 8 face B0 normal[d], 9 edge B0.t1[d],
+// 10 edge B0.t2[d], 11 central8 volume[d], 12 edge length[d],
+// 13 recovery map column q (0..17).
+int gcs_context_debug_array(gcs_context *ctx, int which, int face, int d, int q,
+                            double *out, size_t capacity) {
+  if (!ctx || !out || face < 0 || face >= 6 || d < 0 || d > 2) return -1;
+  gcs::Context &C = ctx->c;
+  const long long nn = C.X.D.Nn;
+  if ((long long)capacity < nn) return -1;
+  const gcs::DevGeom &G = C.X.G;
+  const gcs::DevBg &B = C.X.BG;
+  const double *src = nullptr;
+  const bool bgok = C.bg_pool != nullptr;
+  switch (which) {
+    case 0: src = G.vol; break;
+    case 1: src = G.area[d]; break;
+    case 2: src = G.fn[d][q % 3]; break;
+    case 3: src = G.ft1[d][q % 3]; break;
+    case 4: src = G.ft2[d][q % 3]; break;
+    case 5: src = bgok ? B.b0[q % 3] : nullptr; break;
+    case 6: src = bgok ? B.force[q % 3] : nullptr; break;
+    case 7: src = bgok ? B.fb0[d][q % 3] : nullptr; break;
+    case 8: src = bgok ? B.fb0n[d] : nullptr; break;
+    case 9: src = bgok ? B.eb0t1[d] : nullptr; break;
+    case 10: src = bgok ? B.eb0t2[d] : nullptr; break;
+    case 11: src = G.iv[d]; break;
+    case 12: src = G.elen[d]; break;
+    case 13: src = G.rec[q % 18]; break;
+    default: return -1;
+  }
+  if (!src) return -1;
+  if (cudaMemcpyAsync(out, src + face * nn, nn * sizeof(double),
+                      cudaMemcpyDeviceToHost, C.stream) != cudaSuccess ||
+      cudaStreamSynchronize(C.stream) != cudaSuccess)
+    return -1;
+  return 0;
+}
+
+int gcs_context_dims(const gcs_context *ctx, size_t active[3], size_t *ghost) {
+  if (!ctx || !active || !ghost) return -1;
+  active[0] = (size_t)ctx->c.X.D.nr;
+  active[1] = active[2] = (size_t)ctx->c.X.D.n;
+  *ghost = (size_t)ctx->c.X.D.g;
+  return 0;
 }
 
 void gcs_context_destroy(gcs_context *ctx) {

@@ -7,6 +7,7 @@
 
 #include "gamera_cs_types.h"
 #include "gcs_kernels.cuh"
+#include "gcs_topology.h"
 
 namespace gcs {
 
@@ -46,6 +47,13 @@ struct Context {
   ~Context();
   int init(const gamera_no_grid grid[kFaces], const size_t active[3],
            size_t ghost);
+  // Build a case (kind, sizes, seed) directly on the device
+  // (gcs_build.cu); no host grid is involved.
+  int init_case(int kind, size_t nr, size_t n, unsigned long long seed);
+  int allocate(const size_t active[3], size_t ghost);
+  int allocate_background();
+  int derive();
+  int build_plans(const HaloGeometry &geo);
   void release();
   int upload_background(const gamera_no_background_field bg[kFaces]);
   bool background_matches(const gamera_no_background_field bg[kFaces]) const;

@@ -357,16 +357,79 @@ void Context::set_error(const char *what, const char *where) {
 
 int Context::init(const gamera_no_grid grid[kFaces], const size_t active[3],
                   size_t ghost) {
-  if (active[1] != active[2] || active[1] < 9 || ghost != 4 || active[0] < 1) {
-    set_error("unsupported extents", "init");
-    return -1;
-  }
   for (int f = 0; f < kFaces; ++f)
     for (int a = 0; a < 3; ++a)
       if (grid[f].cell_extent[a] != active[a] + 2 * ghost) {
         set_error("grid extent does not match active + 2 ghost", "init");
         return -1;
       }
+  if (allocate(active, ghost) != 0) return -1;
+  const Dims &D = X.D;
+  DevGeom &G = X.G;
+  for (int f = 0; f < kFaces; ++f) {
+    grid_cell[f] = grid[f].cell;
+    for (int d = 0; d < 3; ++d) grid_face[f][d] = grid[f].face[d].value;
+  }
+  const size_t cells = (size_t)D.E0 * D.E1 * D.E2;
+  // ---- geometry conversion, face by face
+  for (int f = 0; f < kFaces; ++f) {
+    GCS_TRY(cudaMemcpyAsync(staging, grid[f].cell,
+                            cells * sizeof(gamera_no_cell_geometry),
+                            cudaMemcpyHostToDevice, stream));
+    k_conv_cells<<<blocks_for((long long)cells, 128), 128, 0, stream>>>(
+        D, f, (const gamera_no_cell_geometry *)staging, G);
+    for (int d = 0; d < 3; ++d) {
+      const size_t *fe = grid[f].face[d].extent;
+      const size_t fc = fe[0] * fe[1] * fe[2];
+      GCS_TRY(cudaMemcpyAsync(staging, grid[f].face[d].value,
+                              fc * sizeof(gamera_no_face_geometry),
+                              cudaMemcpyHostToDevice, stream));
+      k_conv_faces<<<blocks_for((long long)fc, 128), 128, 0, stream>>>(
+          D, f, d, (const gamera_no_face_geometry *)staging, G);
+      const size_t *ee = grid[f].edge[d].extent;
+      const size_t ec = ee[0] * ee[1] * ee[2];
+      GCS_TRY(cudaMemcpyAsync(staging, grid[f].edge[d].value,
+                              ec * sizeof(gamera_no_edge_geometry),
+                              cudaMemcpyHostToDevice, stream));
+      unsigned char *vbuf = (unsigned char *)staging +
+                            ec * sizeof(gamera_no_edge_geometry);
+      GCS_TRY(cudaMemcpyAsync(vbuf, grid[f].edge[d].valid, ec,
+                              cudaMemcpyHostToDevice, stream));
+      k_conv_edges<<<blocks_for((long long)ec, 128), 128, 0, stream>>>(
+          D, f, d, (const gamera_no_edge_geometry *)staging, vbuf, G);
+    }
+    GCS_TRY(cudaStreamSynchronize(stream));
+  }
+  if (derive() != 0) return -1;
+  // ---- ghost-target geometry of the halo plans, gathered from the grid
+  std::vector<gamera_no_vec3> cc[kFaces], fcen[kFaces][3], farea[kFaces][3];
+  HaloGeometry geo;
+  for (int f = 0; f < kFaces; ++f) {
+    cc[f].resize(cells);
+    for (size_t c = 0; c < cells; ++c) cc[f][c] = grid[f].cell[c].centroid;
+    geo.cell_centroid[f] = cc[f].data();
+    for (int d = 0; d < 3; ++d) {
+      const size_t *fe = grid[f].face[d].extent;
+      const size_t fc = fe[0] * fe[1] * fe[2];
+      fcen[f][d].resize(fc);
+      farea[f][d].resize(fc);
+      for (size_t q = 0; q < fc; ++q) {
+        fcen[f][d][q] = grid[f].face[d].value[q].centroid;
+        farea[f][d][q] = grid[f].face[d].value[q].area_vector;
+      }
+      geo.face_centroid[f][d] = fcen[f][d].data();
+      geo.face_area_vector[f][d] = farea[f][d].data();
+    }
+  }
+  return build_plans(geo);
+}
+
+int Context::allocate(const size_t active[3], size_t ghost) {
+  if (active[1] != active[2] || active[1] < 9 || ghost != 4 || active[0] < 1 ||
+      active[0] > 60000 || active[1] > 60000) {
+    set_error("unsupported extents", "init");
+    return -1;
+  }
   Dims &D = X.D;
   D.nr = (int)active[0];
   D.n = (int)active[1];
@@ -376,9 +439,9 @@ int Context::init(const gamera_no_grid grid[kFaces], const size_t active[3],
   D.N1 = D.E1 + 1;
   D.N2 = D.E2 + 1;
   D.Nn = (long long)(D.E0 + 1) * D.N1 * D.N2;
-  for (int f = 0; f < kFaces; ++f) {
-    grid_cell[f] = grid[f].cell;
-    for (int d = 0; d < 3; ++d) grid_face[f][d] = grid[f].face[d].value;
+  if (D.Nn > 0xffffffffLL) {
+    set_error("more than 2^32 nodes per face", "init");
+    return -1;
   }
   GCS_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
@@ -461,36 +524,13 @@ int Context::init(const gamera_no_grid grid[kFaces], const size_t active[3],
   }
   staging_bytes = largest;
   GCS_TRY(cudaMalloc(&staging, staging_bytes));
+  return 0;
+}
 
-  // ---- geometry conversion, face by face
-  for (int f = 0; f < kFaces; ++f) {
-    GCS_TRY(cudaMemcpyAsync(staging, grid[f].cell,
-                            cells * sizeof(gamera_no_cell_geometry),
-                            cudaMemcpyHostToDevice, stream));
-    k_conv_cells<<<blocks_for((long long)cells, 128), 128, 0, stream>>>(
-        D, f, (const gamera_no_cell_geometry *)staging, G);
-    for (int d = 0; d < 3; ++d) {
-      const size_t *fe = grid[f].face[d].extent;
-      const size_t fc = fe[0] * fe[1] * fe[2];
-      GCS_TRY(cudaMemcpyAsync(staging, grid[f].face[d].value,
-                              fc * sizeof(gamera_no_face_geometry),
-                              cudaMemcpyHostToDevice, stream));
-      k_conv_faces<<<blocks_for((long long)fc, 128), 128, 0, stream>>>(
-          D, f, d, (const gamera_no_face_geometry *)staging, G);
-      const size_t *ee = grid[f].edge[d].extent;
-      const size_t ec = ee[0] * ee[1] * ee[2];
-      GCS_TRY(cudaMemcpyAsync(staging, grid[f].edge[d].value,
-                              ec * sizeof(gamera_no_edge_geometry),
-                              cudaMemcpyHostToDevice, stream));
-      unsigned char *vbuf = (unsigned char *)staging +
-                            ec * sizeof(gamera_no_edge_geometry);
-      GCS_TRY(cudaMemcpyAsync(vbuf, grid[f].edge[d].valid, ec,
-                              cudaMemcpyHostToDevice, stream));
-      k_conv_edges<<<blocks_for((long long)ec, 128), 128, 0, stream>>>(
-          D, f, d, (const gamera_no_edge_geometry *)staging, vbuf, G);
-    }
-    GCS_TRY(cudaStreamSynchronize(stream));
-  }
+// Interface volumes and edge constants from the converted geometry.
+int Context::derive() {
+  const Dims &D = X.D;
+  DevGeom &G = X.G;
   for (int d = 0; d < 3; ++d) {
     const long long fc = (long long)(D.E0 + (d == 0)) * (D.E1 + (d == 1)) *
                          (D.E2 + (d == 2));
@@ -504,14 +544,18 @@ int Context::init(const gamera_no_grid grid[kFaces], const size_t active[3],
   }
   GCS_TRY(cudaGetLastError());
   GCS_TRY(cudaStreamSynchronize(stream));
+  return 0;
+}
 
-  // ---- plans (host), then one device allocation for all of them
+// Host plans, then one device allocation for all of them.
+int Context::build_plans(const HaloGeometry &geo) {
+  const Dims &D = X.D;
   std::vector<HaloCell> hc;
   std::vector<HaloFace> hf;
   std::vector<Seam> seams;
   std::vector<int> offsets;
   std::vector<EdgeMember> members;
-  if (build_halo_cells(grid, D, hc) != 0 || build_halo_faces(grid, D, hf) != 0 ||
+  if (build_halo_cells(geo, D, hc) != 0 || build_halo_faces(geo, D, hf) != 0 ||
       build_seams(D, seams) != 0 ||
       build_edge_groups(D, offsets, members) != 0) {
     set_error("plan construction failed", "init");
@@ -547,29 +591,39 @@ int Context::init(const gamera_no_grid grid[kFaces], const size_t active[3],
   return 0;
 }
 
+void convert_cells(const Ctx &X, int f, const gamera_no_cell_geometry *cells,
+                   cudaStream_t s) {
+  const long long n = (long long)X.D.E0 * X.D.E1 * X.D.E2;
+  k_conv_cells<<<blocks_for(n, 128), 128, 0, s>>>(X.D, f, cells, X.G);
+}
+
+int Context::allocate_background() {
+  const Dims &D = X.D;
+  const long long per = kFaces * D.Nn;
+  std::vector<double **> arrays;
+  DevBg &B = X.BG;
+  for (int q = 0; q < 3; ++q) {
+    arrays.push_back(&B.b0[q]);
+    arrays.push_back(&B.force[q]);
+    arrays.push_back(&B.fb0n[q]);
+    arrays.push_back(&B.eb0t1[q]);
+    arrays.push_back(&B.eb0t2[q]);
+    for (int r = 0; r < 3; ++r) arrays.push_back(&B.fb0[q][r]);
+  }
+  bg_bytes = arrays.size() * per * sizeof(double);
+  GCS_TRY(cudaMalloc(&bg_pool, bg_bytes));
+  GCS_TRY(cudaMemsetAsync(bg_pool, 0, bg_bytes, stream));
+  char *p = (char *)bg_pool;
+  for (double **a : arrays) {
+    *a = (double *)p;
+    p += per * sizeof(double);
+  }
+  return 0;
+}
+
 int Context::upload_background(const gamera_no_background_field bg[kFaces]) {
   const Dims &D = X.D;
-  if (!bg_pool) {
-    const long long per = kFaces * D.Nn;
-    std::vector<double **> arrays;
-    DevBg &B = X.BG;
-    for (int q = 0; q < 3; ++q) {
-      arrays.push_back(&B.b0[q]);
-      arrays.push_back(&B.force[q]);
-      arrays.push_back(&B.fb0n[q]);
-      arrays.push_back(&B.eb0t1[q]);
-      arrays.push_back(&B.eb0t2[q]);
-      for (int r = 0; r < 3; ++r) arrays.push_back(&B.fb0[q][r]);
-    }
-    bg_bytes = arrays.size() * per * sizeof(double);
-    GCS_TRY(cudaMalloc(&bg_pool, bg_bytes));
-    GCS_TRY(cudaMemsetAsync(bg_pool, 0, bg_bytes, stream));
-    char *p = (char *)bg_pool;
-    for (double **a : arrays) {
-      *a = (double *)p;
-      p += per * sizeof(double);
-    }
-  }
+  if (!bg_pool && allocate_background() != 0) return -1;
   const size_t cells = (size_t)D.E0 * D.E1 * D.E2;
   for (int f = 0; f < kFaces; ++f) {
     if (bg[f].cell_magnetic == nullptr) {

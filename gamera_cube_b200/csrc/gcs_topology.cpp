@@ -152,7 +152,7 @@ void linear_weight(double x, long start, int *base, double *fraction) {
 }  // namespace
 
 // cubedsphere_halo.c:401-451, 502-514 (cell targets in the reference order).
-int build_halo_cells(const gamera_no_grid grid[kFaces], const Dims &D,
+int build_halo_cells(const HaloGeometry &geo, const Dims &D,
                      std::vector<HaloCell> &out) {
   out.clear();
   const double qp = 0.25 * acos(-1.0);
@@ -160,12 +160,12 @@ int build_halo_cells(const gamera_no_grid grid[kFaces], const Dims &D,
   const double da = 2.0 * qp / (double)D.n;
   const double db = 2.0 * qp / (double)D.n;
   for (int f = 0; f < kFaces; ++f) {
-    const size_t *ext = grid[f].cell_extent;
+    const size_t ext[3] = {(size_t)D.E0, (size_t)D.E1, (size_t)D.E2};
     for (int i = D.g; i < D.g + D.nr; ++i)
       for (int j = 0; j < D.E1; ++j)
         for (int k = 0; k < D.E2; ++k) {
           if (j >= D.g && j < D.g + D.n && k >= D.g && k < D.g + D.n) continue;
-          const gamera_no_vec3 pt = grid[f].cell[idx3(ext, i, j, k)].centroid;
+          const gamera_no_vec3 pt = geo.cell_centroid[f][idx3(ext, i, j, k)];
           int donor;
           double a, b;
           if (topo::inverse(pt.value, &donor, &a, &b) != 0 || donor == f)
@@ -194,14 +194,16 @@ int build_halo_cells(const gamera_no_grid grid[kFaces], const Dims &D,
 }
 
 // cubedsphere_halo.c:401-451, 515-535 (magnetic ghost faces).
-int build_halo_faces(const gamera_no_grid grid[kFaces], const Dims &D,
+int build_halo_faces(const HaloGeometry &geo, const Dims &D,
                      std::vector<HaloFace> &out) {
   out.clear();
   const double qp = 0.25 * acos(-1.0);
   const long n = D.n;
   for (int f = 0; f < kFaces; ++f) {
     for (int dir = 0; dir < 3; ++dir) {
-      const size_t *ext = grid[f].face[dir].extent;
+      const size_t ext[3] = {(size_t)(D.E0 + (dir == 0)),
+                             (size_t)(D.E1 + (dir == 1)),
+                             (size_t)(D.E2 + (dir == 2))};
       for (size_t i = 0; i < ext[0]; ++i)
         for (size_t j = 0; j < ext[1]; ++j)
           for (size_t k = 0; k < ext[2]; ++k) {
@@ -212,12 +214,12 @@ int build_halo_faces(const gamera_no_grid grid[kFaces], const Dims &D,
               if (coord[d] < (size_t)D.g || coord[d] >= upper) physical = 0;
             }
             if (physical) continue;
-            const gamera_no_face_geometry *geo =
-                &grid[f].face[dir].value[idx3(ext, i, j, k)];
+            const size_t xi = idx3(ext, i, j, k);
+            const gamera_no_vec3 cen = geo.face_centroid[f][dir][xi];
+            const gamera_no_vec3 av = geo.face_area_vector[f][dir][xi];
             int donor;
             double a, b;
-            if (topo::inverse(geo->centroid.value, &donor, &a, &b) != 0)
-              return -1;
+            if (topo::inverse(cen.value, &donor, &a, &b) != 0) return -1;
             const double x = (a + qp) * (double)D.n / (2.0 * qp) - 0.5;
             const double y = (b + qp) * (double)D.n / (2.0 * qp) - 0.5;
             const long sx = stencil_start(x, n), sy = stencil_start(y, n);
@@ -230,9 +232,9 @@ int build_halo_faces(const gamera_no_grid grid[kFaces], const Dims &D,
             HaloFace e;
             e.fx = fx;
             e.fy = fy;
-            e.ax = geo->area_vector.value[0];
-            e.ay = geo->area_vector.value[1];
-            e.az = geo->area_vector.value[2];
+            e.ax = av.value[0];
+            e.ay = av.value[1];
+            e.az = av.value[2];
             e.target = (unsigned)D.node((int)i, (int)j, (int)k);
             e.donor = (unsigned)D.node(si, D.g + (int)sx + bx, D.g + (int)sy + by);
             e.meta = (unsigned)f | ((unsigned)dir << 4) | ((unsigned)donor << 8);

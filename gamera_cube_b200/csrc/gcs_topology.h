@@ -24,10 +24,18 @@ int vertex_key(int face, const size_t active[3], const size_t vertex[3],
 
 }  // namespace topo
 
-// Plans built from the caller's host grid (reference layout).
-int build_halo_cells(const gamera_no_grid grid[kFaces], const Dims &D,
+// Ghost-target geometry the halo plans need, per face: cell centroids over
+// the cell extents and, per face family, face centroids and area vectors
+// over the face extents (reference index order, k contiguous).
+struct HaloGeometry {
+  const gamera_no_vec3 *cell_centroid[kFaces];
+  const gamera_no_vec3 *face_centroid[kFaces][3];
+  const gamera_no_vec3 *face_area_vector[kFaces][3];
+};
+
+int build_halo_cells(const HaloGeometry &geo, const Dims &D,
                      std::vector<HaloCell> &out);
-int build_halo_faces(const gamera_no_grid grid[kFaces], const Dims &D,
+int build_halo_faces(const HaloGeometry &geo, const Dims &D,
                      std::vector<HaloFace> &out);
 int build_seams(const Dims &D, std::vector<Seam> &out);
 int build_edge_groups(const Dims &D, std::vector<int> &offsets,

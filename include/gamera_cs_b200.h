@@ -122,6 +122,31 @@ gcs_context *gcs_context_create(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
                                 const size_t active[3], size_t ghost);
 void gcs_context_destroy(gcs_context *ctx);
 const char *gcs_last_error(void);
+
+/* Build a case directly in device memory (no host grid): kind 0 uniform MHD
+ * state (r in [2, 2.5]), 1 radial MHD shock (r in [2, 3]), 2 solar wind
+ * with aligned dipole B0 and seeded +-1% density noise (log-stretched r in
+ * [2.5, 30] R_E), 3 the wind with a 20% density pulse; nr radial and n
+ * angular active cells per face, 4 ghosts.  Same inputs as the oracle's
+ * case set up to device-libm rounding. */
+gcs_context *gcs_context_create_case(int kind, size_t nr, size_t n,
+                                     unsigned long long seed);
+/* Step, CFL and driver options of a case kind. */
+int gcs_case_options(int kind, gamera_no_advance_options *options,
+                     gamera_no_timestep_options *timestep);
+int gcs_context_dims(const gcs_context *ctx, size_t active[3], size_t *ghost);
+/* Diagnostics: copy one device geometry/background node array of one face
+ * (nodes_per_face = (nr+9)(n+9)^2 doubles, padded node index) to out. */
+int gcs_context_debug_array(gcs_context *ctx, int which, int face, int d, int q,
+                            double *out, size_t capacity);
+/* The drop-in step of gamera_cs_advance_six_with_background_planned on
+ * host storage (state uploaded before, downloaded after the step) for a
+ * context built by gcs_context_create_case, which owns its grid and
+ * background. */
+int gcs_context_advance_host(gcs_context *ctx,
+                             gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                             const gamera_no_advance_options *options,
+                             double predictor_ratio, double dt);
 const char *gcs_context_error(const gcs_context *ctx);
 
 int gcs_context_upload_background(

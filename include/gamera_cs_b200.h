@@ -199,6 +199,36 @@ int gcs_context_stage_times(gcs_context *ctx, double *ms, long long *calls,
                             int capacity);
 const char *gcs_stage_name(int stage_slot);
 size_t gcs_context_device_bytes(const gcs_context *ctx);
+/* Allocation-free CFL time step.  No counterpart in the reference: an
+ * addition for callers that cannot call cudaMalloc when they need the step
+ * (device arrays owned by another allocator or runtime, or a driver that
+ * forbids device allocation after start-up).  Inputs are caller-owned
+ * DEVICE arrays in the reference layout (cells: gamera_no_cell_geometry per
+ * cell; conserved: 5 doubles per cell; cell and background B: one vec3 per
+ * cell, NULL where the options do not use them); the minimum over the
+ * active box of the reference cell step (the quantity
+ * gamera_no_local_timestep computes) is returned in *local_dt on the host.
+ * No device memory is allocated or freed: the reduction uses a static
+ * device array of gcs_noalloc_scratch_bytes() bytes (about 768 KiB) that
+ * every GPU loading this library holds until exit.  At most 16,777,216
+ * active cells per call; larger boxes are rejected with -1 and a message in
+ * gcs_noalloc_last_error().  The first call on each device looks up the
+ * array's device address, so make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised.  Runs on the default stream and returns after the result is
+ * on the host. */
+int gcs_local_timestep_noalloc(const size_t cell_extent[3],
+                               const gamera_no_cell_geometry *cells,
+                               const double *conserved,
+                               const gamera_no_vec3 *cell_magnetic,
+                               const gamera_no_vec3 *background_cell_magnetic,
+                               const size_t active_lower[3],
+                               const size_t active_upper[3],
+                               const gamera_no_timestep_options *options,
+                               double *local_dt);
+const char *gcs_noalloc_last_error(void);
+size_t gcs_noalloc_scratch_bytes(void);
+
 /* Resident mode: the device copy stays authoritative between drop-in calls
  * made with the same storage pointer; gcs_context_download_state copies it
  * back explicitly. */

@@ -44,6 +44,9 @@ struct DevState {
   double *B[3], *Bo[3];          // residual cell B, old (cells)
   double *P[3], *Po[3];          // face magnetic flux per face family
   double *Up[5], *Bp[3], *Pp[3]; // predictor outputs
+  double *Pr[5];                 // primitives of Up (sweep options); rho NaN
+                                 // where the conversion fails
+  double *BN[3];                 // Pp / face area per face family
   double *W[3];                  // (V * m_c) / max(rho, floor) per cell
   double *FV[3][3];              // face velocity per face family, 3 comps
   double *F[3][5];               // area-scaled fluid flux per face family

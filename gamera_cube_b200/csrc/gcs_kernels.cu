@@ -266,7 +266,11 @@ __global__ void k_halo_faces(Dims D, const HaloFace *plan, long long count,
 // (nonorthogonal_step.c:379-419): U~ = prim^-1(P + r (P - P_old)),
 // Phi~ = Phi + r (Phi - Phi_old), B~ = recover(Phi~); plus the per-cell
 // momentum weights (V m)/max(rho, floor) of the EMF face velocities
-// (nonorthogonal_sweep.c:223-249), which depend on U~ only.
+// (nonorthogonal_sweep.c:223-249), which depend on U~ only.  Also stores,
+// once per cell and face, two quantities every sweep stencil reads many
+// times: the primitive state of U~ under the sweep options
+// (nonorthogonal_sweep.c:144-149, rho = NaN marks a failed conversion) and
+// the face-normal field Phi~ / area (nonorthogonal_sweep.c:466-467, 391).
 __global__ void k_predict(Dims D, DevState S, DevGeom G, Opts O,
                           const StepParams *prm, DevStatus *st) {
   if (failed(st)) return;
@@ -283,7 +287,11 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Opts O,
 #pragma unroll
     for (int a = 0; a < 3; ++a)
       in = in && coord[a] < D.ext(a) + (a == d ? 1 : 0);
-    if (in) S.Pp[d][c] = S.P[d][c] + r * (S.P[d][c] - S.Po[d][c]);
+    if (in) {
+      const double pp = S.P[d][c] + r * (S.P[d][c] - S.Po[d][c]);
+      S.Pp[d][c] = pp;
+      S.BN[d][c] = pp / G.area[d][c];
+    }
   }
   if (!cell) return;
   double uo[5], uc[5], up[5];
@@ -298,6 +306,13 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Opts O,
   }
 #pragma unroll
   for (int m = 0; m < 5; ++m) S.Up[m][c] = up[m];
+  Prim pr;
+  if (cons_to_prim(up, O.s_gamma, O.s_rho_floor, O.s_p_floor, &pr)) pr.rho = NAN;
+  S.Pr[0][c] = pr.rho;
+  S.Pr[1][c] = pr.vx;
+  S.Pr[2][c] = pr.vy;
+  S.Pr[3][c] = pr.vz;
+  S.Pr[4][c] = pr.p;
   const double v = G.vol[c];
   const double rho = fmax(up[0], O.e_rho_floor);
 #pragma unroll
@@ -320,52 +335,56 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Opts O,
 
 // ---------------------------------------------------------------------------
 // Face-flux sweep in direction d (nonorthogonal_sweep.c:408-548).
+// Each thread owns one face; the eight-cell stencil of one variable at a
+// time is read from the predictor's cell primitives, so only the volumes,
+// one stencil and the reconstructed face states are live at once.
 template <int d>
-__global__ void __launch_bounds__(128) k_flux(Dims D, DevState S, DevGeom G,
-                                              DevBg BG, Opts O,
-                                              DevStatus *st) {
+__global__ void __launch_bounds__(128, 4) k_flux(Dims D, DevState S, DevGeom G,
+                                                 DevBg BG, Opts O,
+                                                 DevStatus *st) {
   if (failed(st)) return;
   int f, i, j, k;
   const Box b{D.g, D.g, D.g, D.n + (d == 1), D.n + (d == 2)};
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const long long c = f * D.Nn + D.node(i, j, k);
   const long long sd = D.stride(d);
-  double vol[8];
-  Prim pr[8];
-#pragma unroll
-  for (int n = 0; n < 8; ++n) {
-    const long long x = c + (n - 4) * sd;
-    vol[n] = G.vol[x];
-    double u[5];
-#pragma unroll
-    for (int m = 0; m < 5; ++m) u[m] = S.Up[m][x];
-    if (cons_to_prim(u, O.s_gamma, O.s_rho_floor, O.s_p_floor, &pr[n])) {
-      fail(st, kStageReconstruct, d, f, i, j, k);
-      return;
-    }
-  }
   const double iv = G.iv[d][c];
+  if (isnan(iv)) {
+    fail(st, kStageReconstruct, d, f, i, j, k);
+    return;
+  }
+  double vol[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) vol[n] = G.vol[c + (n - 4) * sd];
   Prim st2[2];
   {
     double q[8], l, r;
+    bool ok = true;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = pr[n].rho;
+    for (int n = 0; n < 8; ++n) {
+      q[n] = S.Pr[0][c + (n - 4) * sd];
+      ok = ok && !isnan(q[n]);
+    }
+    if (!ok) {
+      fail(st, kStageReconstruct, d, f, i, j, k);
+      return;
+    }
     up7_pdm(vol, q, iv, O.pdm, &l, &r);
     st2[0].rho = l; st2[1].rho = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = pr[n].vx;
+    for (int n = 0; n < 8; ++n) q[n] = S.Pr[1][c + (n - 4) * sd];
     up7_pdm(vol, q, iv, O.pdm, &l, &r);
     st2[0].vx = l; st2[1].vx = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = pr[n].vy;
+    for (int n = 0; n < 8; ++n) q[n] = S.Pr[2][c + (n - 4) * sd];
     up7_pdm(vol, q, iv, O.pdm, &l, &r);
     st2[0].vy = l; st2[1].vy = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = pr[n].vz;
+    for (int n = 0; n < 8; ++n) q[n] = S.Pr[3][c + (n - 4) * sd];
     up7_pdm(vol, q, iv, O.pdm, &l, &r);
     st2[0].vz = l; st2[1].vz = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = pr[n].p;
+    for (int n = 0; n < 8; ++n) q[n] = S.Pr[4][c + (n - 4) * sd];
     up7_pdm(vol, q, iv, O.pdm, &l, &r);
     st2[0].p = l; st2[1].p = r;
   }
@@ -388,11 +407,10 @@ __global__ void __launch_bounds__(128) k_flux(Dims D, DevState S, DevGeom G,
     fail(st, kStageKineticFluid, d, f, i, j, k);
     return;
   }
-  const double area = G.area[d][c];
   MaxwellFlux mx;
   mx.m[0] = mx.m[1] = mx.m[2] = 0.0;
   if (O.s_mhd) {
-    const double bn = S.Pp[d][c] / area;
+    const double bn = S.BN[d][c];
     double b0[3] = {0.0, 0.0, 0.0};
     double b0n = 0.0;
     if (O.s_bg) {
@@ -427,6 +445,7 @@ __global__ void __launch_bounds__(128) k_flux(Dims D, DevState S, DevGeom G,
       }
     }
   }
+  const double area = G.area[d][c];
 #pragma unroll
   for (int m = 0; m < 5; ++m) S.F[d][m][c] = area * fl.f[m];
 #pragma unroll
@@ -503,13 +522,13 @@ __global__ void __launch_bounds__(128) k_edge_emf(Dims D, DevState S,
   // transverse face fields (nonorthogonal_sweep.c:372-406)
   double fl, fr, sl, sr;
 #pragma unroll
-  for (int n = 0; n < 8; ++n) fld[n] = S.Pp[a][c + (n - 4) * sb] / ar[n];
+  for (int n = 0; n < 8; ++n) fld[n] = S.BN[a][c + (n - 4) * sb];
   up7_pdm(ar, fld, ca, O.e_pdm, &fl, &fr);
   double ar2[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     ar2[n] = G.area[bb][c + (n - 4) * sa];
-    fld[n] = S.Pp[bb][c + (n - 4) * sa] / ar2[n];
+    fld[n] = S.BN[bb][c + (n - 4) * sa];
   }
   up7_pdm(ar2, fld, G.cb[e][c], O.e_pdm, &sl, &sr);
   // 2x2 edge solve (nonorthogonal_operators.c:56-79)

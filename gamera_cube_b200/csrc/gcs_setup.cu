@@ -455,7 +455,9 @@ int Context::allocate(const size_t active[3], size_t ghost) {
     arrays.push_back(&S.U[m]);
     arrays.push_back(&S.Uo[m]);
     arrays.push_back(&S.Up[m]);
+    arrays.push_back(&S.Pr[m]);
   }
+  for (int m = 0; m < 3; ++m) arrays.push_back(&S.BN[m]);
   for (int m = 0; m < 3; ++m) {
     arrays.push_back(&S.B[m]);
     arrays.push_back(&S.Bo[m]);

@@ -353,6 +353,7 @@ __global__ void __launch_bounds__(128, 4) k_flux(Dims D, DevState S, DevGeom G,
     fail(st, kStageReconstruct, d, f, i, j, k);
     return;
   }
+  const double riv = 1.0 / iv;
   double vol[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) vol[n] = G.vol[c + (n - 4) * sd];
@@ -369,23 +370,23 @@ __global__ void __launch_bounds__(128, 4) k_flux(Dims D, DevState S, DevGeom G,
       fail(st, kStageReconstruct, d, f, i, j, k);
       return;
     }
-    up7_pdm(vol, q, iv, O.pdm, &l, &r);
+    up7_pdm_rcp(vol, q, riv, O.pdm, &l, &r);
     st2[0].rho = l; st2[1].rho = r;
 #pragma unroll
     for (int n = 0; n < 8; ++n) q[n] = S.Pr[1][c + (n - 4) * sd];
-    up7_pdm(vol, q, iv, O.pdm, &l, &r);
+    up7_pdm_rcp(vol, q, riv, O.pdm, &l, &r);
     st2[0].vx = l; st2[1].vx = r;
 #pragma unroll
     for (int n = 0; n < 8; ++n) q[n] = S.Pr[2][c + (n - 4) * sd];
-    up7_pdm(vol, q, iv, O.pdm, &l, &r);
+    up7_pdm_rcp(vol, q, riv, O.pdm, &l, &r);
     st2[0].vy = l; st2[1].vy = r;
 #pragma unroll
     for (int n = 0; n < 8; ++n) q[n] = S.Pr[3][c + (n - 4) * sd];
-    up7_pdm(vol, q, iv, O.pdm, &l, &r);
+    up7_pdm_rcp(vol, q, riv, O.pdm, &l, &r);
     st2[0].vz = l; st2[1].vz = r;
 #pragma unroll
     for (int n = 0; n < 8; ++n) q[n] = S.Pr[4][c + (n - 4) * sd];
-    up7_pdm(vol, q, iv, O.pdm, &l, &r);
+    up7_pdm_rcp(vol, q, riv, O.pdm, &l, &r);
     st2[0].p = l; st2[1].p = r;
   }
   double mag[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
@@ -395,7 +396,7 @@ __global__ void __launch_bounds__(128, 4) k_flux(Dims D, DevState S, DevGeom G,
       double q[8];
 #pragma unroll
       for (int n = 0; n < 8; ++n) q[n] = S.Bp[m][c + (n - 4) * sd];
-      up7_pdm(vol, q, iv, O.pdm, &mag[0][m], &mag[1][m]);
+      up7_pdm_rcp(vol, q, riv, O.pdm, &mag[0][m], &mag[1][m]);
     }
   }
   FaceFrame fr;
@@ -469,13 +470,13 @@ __global__ void k_face_velocity(Dims D, DevState S, DevGeom G, DevStatus *st) {
   if (!box_coord(b, &f, &x[0], &x[1], &x[2])) return;
   const long long c = f * D.Nn + D.node(x[0], x[1], x[2]);
   const long long sa = D.stride(a);
-  const double iv = G.iv[a][c];
+  const double riv = 1.0 / G.iv[a][c];
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     double w[8];
 #pragma unroll
     for (int n = 0; n < 8; ++n) w[n] = S.W[m][c + (n - 4) * sa];
-    S.FV[a][m][c] = central8(w) / iv;
+    S.FV[a][m][c] = central8(w) * riv;
   }
 }
 
@@ -507,13 +508,13 @@ __global__ void __launch_bounds__(128) k_edge_emf(Dims D, DevState S,
   double v[3];
 #pragma unroll
   for (int n = 0; n < 8; ++n) ar[n] = G.area[a][c + (n - 4) * sb];
-  const double ca = G.ca[e][c];
+  const double rca = 1.0 / G.ca[e][c];
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     double w[8];
 #pragma unroll
     for (int n = 0; n < 8; ++n) w[n] = ar[n] * S.FV[a][m][c + (n - 4) * sb];
-    v[m] = central8(w) / ca;
+    v[m] = central8(w) * rca;
   }
   const double vt1 =
       dot3(v[0], v[1], v[2], G.et1[e][0][c], G.et1[e][1][c], G.et1[e][2][c]);
@@ -523,14 +524,14 @@ __global__ void __launch_bounds__(128) k_edge_emf(Dims D, DevState S,
   double fl, fr, sl, sr;
 #pragma unroll
   for (int n = 0; n < 8; ++n) fld[n] = S.BN[a][c + (n - 4) * sb];
-  up7_pdm(ar, fld, ca, O.e_pdm, &fl, &fr);
+  up7_pdm_rcp(ar, fld, rca, O.e_pdm, &fl, &fr);
   double ar2[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     ar2[n] = G.area[bb][c + (n - 4) * sa];
     fld[n] = S.BN[bb][c + (n - 4) * sa];
   }
-  up7_pdm(ar2, fld, G.cb[e][c], O.e_pdm, &sl, &sr);
+  up7_pdm_rcp(ar2, fld, 1.0 / G.cb[e][c], O.e_pdm, &sl, &sr);
   // 2x2 edge solve (nonorthogonal_operators.c:56-79)
   const double f1 = 0.5 * (fl + fr);
   const double f2 = 0.5 * (sl + sr);

@@ -107,6 +107,22 @@ __host__ __device__ inline void up7_pdm(const double vol[8], const double q[8],
   *right = pdm_left(q[5], q[4], q[3], hr, pdmb);
 }
 
+// up7_pdm with the division by the interface volume replaced by a multiply
+// with its reciprocal (computed once per face for all eight variables):
+// the high-order value may differ from the reference's by one rounding.
+__host__ __device__ inline void up7_pdm_rcp(const double vol[8],
+                                            const double q[8], double riv,
+                                            double pdmb, double *left,
+                                            double *right) {
+  double w[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) w[n] = vol[n] * q[n];
+  const double hl = upwind7_left(w) * riv;
+  const double hr = upwind7_right(w) * riv;
+  *left = pdm_left(q[2], q[3], q[4], hl, pdmb);
+  *right = pdm_left(q[5], q[4], q[3], hr, pdmb);
+}
+
 // nonorthogonal_state.c:60-93
 __host__ __device__ inline int cons_to_prim(const double u[5], double gamma,
                                             double rho_floor, double p_floor,

@@ -242,6 +242,8 @@ def run_gpu(args):
     barrier(dist, device)
     e2e_value = total_cells * e2e_steps / e2e_s
 
+    mi = run_mi(lib, torch, device, args.mi_solves) if args.mi_solves > 0 else None
+
     result = None
     if rank == 0:
         clk = clocks.summary()
@@ -268,6 +270,8 @@ def run_gpu(args):
                        "parallelism": "replicas x%d" % world,
                        "setup_s": round(setup_s, 2)},
             "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches_note": "MHD step graph only; each MI solve is one "
+                                 "launch (timed separately under \"mi\")",
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": hs.bytes_state,
@@ -285,13 +289,148 @@ def run_gpu(args):
                          (ms_local / args.steps * 1e-3) / 1e9 / hbm},
             "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         }
+        if mi is not None:
+            result["mi"] = mi
         if args.cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(args)
+            if mi is not None:
+                result["mi"]["cpu_baseline"] = mi_cpu_baseline()
     lib.gcs_context_destroy(ctx)
     if dist is not None:
         dist.destroy_process_group()
     if result is not None:
         print(json.dumps(result))
+
+
+MI_GRID = (361, 181)            # longitudes, colatitudes per hemisphere
+MI_SEED = 2024
+# Algorithmic bytes of one PCG iteration if its vectors streamed from memory:
+# about 20 FP64 vector touches per unknown.
+MI_BYTES_PER_UNKNOWN_ITER = 160
+
+
+def mi_cases():
+    from gamera_cube_b200 import cases
+    npl, nt = MI_GRID
+    return [cases.mi_case(npl, nt, seed=MI_SEED, hemisphere=h)
+            for h in (cases.NORTH, cases.SOUTH)]
+
+
+def run_mi(lib, torch, device, solves):
+    """Constant-Pedersen ionosphere solves on the 181 x 361 polar cap
+    (colatitude 0-45 deg), rel. residual 1e-8, zero initial guess: one
+    hemisphere per call, and both hemispheres in one launch.  Device time
+    with CUDA events around each solve; L2 flushed between solves."""
+    import numpy as np
+    from gamera_cube_b200 import abi
+    cs = mi_cases()
+    npl, nt = MI_GRID
+    nodes = npl * nt
+    unknowns = 1 + npl * (nt - 2)
+    fac = torch.from_numpy(np.concatenate([c.fac.ravel() for c in cs])).to(device)
+    pot = torch.zeros(2 * nodes, dtype=torch.float64, device=device)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    out = {}
+    for label, count in (("one", 1), ("pair", 2)):
+        cfgs = (abi.MiSolverConfig * count)(*[c.config for c in cs[:count]])
+        plan = C.c_void_p()
+        if lib.gcs_mi_plan_create(cfgs, count, C.byref(plan)) != 0:
+            raise RuntimeError(lib.gcs_last_error().decode())
+        stats = (abi.MiSolverStats * count)()
+        status = (C.c_int * count)()
+        times = []
+        stream = torch.cuda.current_stream(device)
+        for q in range(3 + solves):
+            pot.zero_()
+            flush.fill_(float(q))
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            if lib.gcs_mi_solve_constant_pedersen_async(
+                    plan, C.c_void_p(fac.data_ptr()), C.c_void_p(pot.data_ptr()),
+                    C.c_void_p(stream.cuda_stream)) != 0:
+                raise RuntimeError(lib.gcs_last_error().decode())
+            ev1.record(stream)
+            if lib.gcs_mi_plan_results(plan, stats, status) != 0:
+                raise RuntimeError(lib.gcs_last_error().decode())
+            if any(status[h] != 0 for h in range(count)):
+                raise RuntimeError("MI solve did not converge")
+            if q >= 3:
+                times.append(ev0.elapsed_time(ev1))
+        csize = C.c_int()
+        lib.gcs_mi_plan_info(plan, C.byref(csize), None, None)
+        lib.gcs_mi_plan_destroy(plan)
+        out[label] = (sorted(times)[len(times) // 2], [stats[h].iterations
+                                                       for h in range(count)],
+                      csize.value)
+    # end to end through the drop-in (host arrays, copies inside)
+    c0 = cs[0]
+    e2e = []
+    for q in range(3 + solves):
+        guess = np.zeros((nt, npl))
+        st = abi.MiSolverStats()
+        torch.cuda.synchronize(device)
+        t = time.perf_counter()
+        rc = lib.gamera_mi_solve_constant_pedersen(
+            C.byref(c0.config), c0.fac.ctypes.data_as(C.POINTER(C.c_double)),
+            guess.ctypes.data_as(C.POINTER(C.c_double)), C.byref(st))
+        e2e_ms = (time.perf_counter() - t) * 1e3
+        if rc != 0:
+            raise RuntimeError("drop-in MI solve failed")
+        if q >= 3:
+            e2e.append(e2e_ms)
+    ms_one, it_one, csize = out["one"]
+    ms_pair, it_pair, _ = out["pair"]
+    us_iter = ms_one * 1e3 / it_one[0]
+    eff = MI_BYTES_PER_UNKNOWN_ITER * unknowns / (us_iter * 1e-6) / 1e9
+    return {
+        "workload": "ionosphere potential, %d colat x %d lon polar cap (0-45 deg), "
+                    "constant Pedersen 5 S, R1/R2 FAC +-1 uA/m^2 + noise, "
+                    "rel. residual 1e-8, zero initial guess" % (nt, npl),
+        "unknowns_per_hemisphere": unknowns,
+        "ms_per_call": ms_one,
+        "ms_per_call_both_hemispheres_one_launch": ms_pair,
+        "iterations": it_pair,
+        "us_per_iteration": us_iter,
+        "cluster_ctas": csize,
+        "e2e_ms_per_call": sorted(e2e)[len(e2e) // 2],
+        "e2e_call": "gamera_mi_solve_constant_pedersen (drop-in, host arrays, "
+                    "H2D/D2H of %d B each way)" % (2 * nodes * 8),
+        "effective_gbs": eff,
+        "bound": "latency (3 cluster barriers per iteration; vectors on chip)",
+        "solves_timed": solves,
+    }
+
+
+def mi_cpu_baseline():
+    """The reference's constant-Pedersen and tensor solves (oracle/_ref, one
+    thread: the reference MI solver is serial) on the north hemisphere."""
+    from oracle import refbind
+    from gamera_cube_b200 import abi, cases
+    if not refbind.ref_available():
+        return None
+    lib = refbind.ref()
+    c = mi_cases()[0]
+    P = C.POINTER(C.c_double)
+    pot = c.potential.copy()
+    st = abi.MiSolverStats()
+    t = time.perf_counter()
+    rc = lib.gamera_mi_solve_constant_pedersen(C.byref(c.config), c.fac.ctypes.data_as(P),
+                                               pot.ctypes.data_as(P), C.byref(st))
+    const_ms = (time.perf_counter() - t) * 1e3
+    npl, nt = MI_GRID
+    tcfg = cases.mi_config(npl, nt, max_iterations=20000)
+    pot = c.potential.copy()
+    st2 = abi.MiSolverStats()
+    t = time.perf_counter()
+    rc2 = lib.gamera_mi_solve_conductance_tensor(
+        C.byref(tcfg), c.fac.ctypes.data_as(P), c.pedersen.ctypes.data_as(P),
+        c.hall.ctypes.data_as(P), pot.ctypes.data_as(P), C.byref(st2))
+    tensor_ms = (time.perf_counter() - t) * 1e3
+    return {"ms_per_call": const_ms, "iterations": st.iterations, "converged": rc == 0,
+            "tensor_ms_per_call": tensor_ms, "tensor_iterations": st2.iterations,
+            "tensor_converged": rc2 == 0, "cores": 1, "kind": "reference",
+            "sample": "one north-hemisphere call of each solver"}
 
 
 def _ref_bench_path():
@@ -351,6 +490,8 @@ def run_reference(args):
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": base["unit"],
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.mi_solves > 0:
+        line["mi"] = mi_cpu_baseline()
     print(json.dumps(line))
 
 
@@ -366,6 +507,8 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=16)
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--mi-solves", type=int, default=10,
+                    help="timed ionosphere solves (0 skips the MI measurement)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

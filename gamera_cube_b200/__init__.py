@@ -81,6 +81,25 @@ def _load():
         "gcs_context_debug_array": (C.c_int, [C.c_void_p, C.c_int, C.c_int,
                                               C.c_int, C.c_int, P(C.c_double),
                                               C.c_size_t]),
+        "gamera_mi_apply_constant_pedersen": (
+            C.c_int, [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double)]),
+        "gamera_mi_solve_constant_pedersen": (
+            C.c_int, [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double),
+                      P(abi.MiSolverStats)]),
+        "gamera_mi_apply_conductance_tensor": (
+            C.c_int, [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double),
+                      P(C.c_double), P(C.c_double)]),
+        "gcs_mi_plan_create": (C.c_int, [P(abi.MiSolverConfig), C.c_int,
+                                         P(C.c_void_p)]),
+        "gcs_mi_plan_destroy": (None, [C.c_void_p]),
+        "gcs_mi_plan_info": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int),
+                                       P(C.c_size_t)]),
+        "gcs_mi_plan_buffers": (C.c_int, [C.c_void_p, P(C.c_void_p),
+                                          P(C.c_void_p)]),
+        "gcs_mi_solve_constant_pedersen_async": (
+            C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "gcs_mi_plan_results": (C.c_int, [C.c_void_p, P(abi.MiSolverStats),
+                                          P(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

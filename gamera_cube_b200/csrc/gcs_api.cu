@@ -399,6 +399,10 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
 
 }  // namespace
 
+namespace gcs {
+void set_api_error(const char *msg) { set_last(msg); }
+}  // namespace gcs
+
 extern "C" {
 
 // ------------------------------------------------------------------ Part 1

@@ -88,6 +88,24 @@ int gamera_cs_fill_magnetic_face_halos_planned(
 /* cubedsphere/cubedsphere_halo.h:32 */
 int gamera_cs_halo_valid_state(const double state[GAMERA_NO_FLUX_COUNT]);
 
+/* Ionosphere potential solves, host arrays in the reference layout
+ * (theta-major, longitude contiguous), synchronous.  The constant-Pedersen
+ * solve runs on the GPU; its stats count the GPU's own iterations (dot
+ * products are summed in a fixed parallel order, so the iteration count may
+ * differ from the CPU solver's by a few and the potential agrees to the
+ * solver tolerance).  The apply functions are bitwise the reference's.
+ * nonorthogonal/src/nonorthogonal/nonorthogonal_mi.h:70-72 */
+int gamera_mi_apply_constant_pedersen(const gamera_mi_solver_config *config,
+                                      const double *potential_v, double *result);
+/* nonorthogonal_mi.h:81-83 */
+int gamera_mi_solve_constant_pedersen(const gamera_mi_solver_config *config,
+                                      const double *fac_a_m2, double *potential_v,
+                                      gamera_mi_solver_stats *stats);
+/* nonorthogonal_mi.h:95-98 */
+int gamera_mi_apply_conductance_tensor(const gamera_mi_solver_config *config,
+                                       const double *pedersen, const double *hall,
+                                       const double *potential_v, double *result);
+
 /* ---------------------------------------------------------------- Part 2 */
 
 typedef struct gcs_context gcs_context;
@@ -234,6 +252,29 @@ size_t gcs_noalloc_scratch_bytes(void);
  * back explicitly. */
 gcs_context *gcs_halo_plan_context(gamera_cs_halo_plan *plan);
 int gcs_context_set_resident(gcs_context *ctx, int on);
+
+/* Device-resident ionosphere solves (no reference counterpart).  A plan
+ * holds `count` independent systems on one polar grid (for example the two
+ * hemispheres, configs differing in `hemisphere`); one solve launch runs
+ * them concurrently, one thread-block cluster each, entirely on chip.
+ * Arrays are count x colatitude_count x longitude_count doubles in device
+ * memory; NULL selects the plan's own buffers (gcs_mi_plan_buffers).  The
+ * launch is asynchronous on `stream` (a cudaStream_t, NULL = default);
+ * gcs_mi_plan_results waits for it and returns per-system stats and status
+ * (0 converged, 1 not converged, 2 non-finite FAC: potential untouched).
+ * Grids up to about 100,000 unknowns per system are supported; larger ones
+ * fail at plan creation.  maximum_iterations is clamped to 1,048,576. */
+typedef struct gcs_mi_plan gcs_mi_plan;
+int gcs_mi_plan_create(const gamera_mi_solver_config *configs, int count,
+                       gcs_mi_plan **plan);
+void gcs_mi_plan_destroy(gcs_mi_plan *plan);
+int gcs_mi_plan_info(const gcs_mi_plan *plan, int *cluster_ctas,
+                     int *threads_per_cta, size_t *shared_bytes);
+int gcs_mi_plan_buffers(gcs_mi_plan *plan, double **fac, double **potential);
+int gcs_mi_solve_constant_pedersen_async(gcs_mi_plan *plan, const double *fac,
+                                         double *potential, void *stream);
+int gcs_mi_plan_results(gcs_mi_plan *plan, gamera_mi_solver_stats *stats,
+                        int *status);
 
 #ifdef __cplusplus
 }

@@ -397,7 +397,7 @@ def run_mi(lib, torch, device, solves):
         "e2e_call": "gamera_mi_solve_constant_pedersen (drop-in, host arrays, "
                     "H2D/D2H of %d B each way)" % (2 * nodes * 8),
         "effective_gbs": eff,
-        "bound": "latency (3 cluster barriers per iteration; vectors on chip)",
+        "bound": "latency (2 cluster barriers per iteration; vectors on chip)",
         "solves_timed": solves,
     }
 

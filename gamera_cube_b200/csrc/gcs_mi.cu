@@ -40,7 +40,6 @@ namespace gcs {
 namespace mi {
 
 constexpr int kThreads = 512;
-constexpr int kWarps = kThreads / 32;
 constexpr int kMaxCluster = 16;
 constexpr int kPortableCluster = 8;
 constexpr int kSlots = 4;       // rotating cluster-reduction slots
@@ -88,67 +87,86 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Sum of N values over the CTA; every thread receives the same result.
+// Warp butterflies, then lane w of every warp takes warp w's partial and a
+// second butterfly combines them: each warp runs the identical sequence of
+// additions, so all threads hold bit-identical sums.
 template <int N>
 __device__ __forceinline__ void block_sum(double (&v)[N], double *wbuf) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
 #pragma unroll
   for (int q = 0; q < N; ++q) {
     v[q] = warp_sum(v[q]);
-    if (lane == 0) wbuf[warp * N + q] = v[q];
+    if (lane == 0) wbuf[warp * kSlotWidth + q] = v[q];
   }
   __syncthreads();
 #pragma unroll
-  for (int q = 0; q < N; ++q) {
-    double a = 0.0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) a += wbuf[w * N + q];
-    v[q] = a;
-  }
+  for (int q = 0; q < N; ++q)
+    v[q] = warp_sum(lane < nwarps ? wbuf[lane * kSlotWidth + q] : 0.0);
 }
 
-// Sum of each CTA's N values over the cluster, in rank order.  The cluster
-// barrier also publishes every shared-memory write made before it.
+// Sum of each CTA's N values over the cluster, in rank order.  Thread c
+// pushes this CTA's values into CTA c's slot table (a store into distributed
+// shared memory, so no thread waits on a remote load); after the cluster
+// barrier -- which also publishes every shared-memory write made before it
+// -- lane c of every warp reads rank c's entry locally and a warp butterfly
+// sums them, so all CTAs hold bit-identical sums.
 template <int N>
 __device__ __forceinline__ void cluster_sum(cg::cluster_group &cl, double (&v)[N],
-                                            double *slots, int &ctr, int csize) {
+                                            double *slots, int &ctr, int rank,
+                                            int csize) {
   const int slot = ctr & (kSlots - 1);
   ++ctr;
-  if (threadIdx.x == 0) {
+  if ((int)threadIdx.x < csize) {
+    double *dst = cl.map_shared_rank(slots, (int)threadIdx.x) +
+                  (slot * kMaxCluster + rank) * kSlotWidth;
 #pragma unroll
-    for (int q = 0; q < N; ++q) slots[slot * kSlotWidth + q] = v[q];
+    for (int q = 0; q < N; ++q) dst[q] = v[q];
   }
   cl.sync();
+  const int lane = threadIdx.x & 31;
+  const double *src = slots + slot * kMaxCluster * kSlotWidth;
 #pragma unroll
-  for (int q = 0; q < N; ++q) v[q] = 0.0;
-  for (int c = 0; c < csize; ++c) {
-    const double *rs = cl.map_shared_rank(slots, c);
-#pragma unroll
-    for (int q = 0; q < N; ++q) v[q] += rs[slot * kSlotWidth + q];
-  }
+  for (int q = 0; q < N; ++q)
+    v[q] = warp_sum(lane < csize ? src[lane * kSlotWidth + q] : 0.0);
 }
 
+// A CTA's band of rows plus copies of the adjacent rows of the neighbouring
+// bands (hs: search direction, hz: preconditioned residual), kept current by
+// the owners' pushes.
 struct Band {
-  int ra, nrow;            // first interior row (0-based) and row count
-  const double *up;        // neighbour band above (rank - 1), or null
-  const double *dn;        // neighbour band below (rank + 1), or null
-  int up_last;             // offset of the above band's last row
+  int ra, nrow;        // first interior row (0-based) and row count
+  bool top, bottom;    // band holds the first / the last interior row
+  double *hs_up, *hz_up;   // row above the band (last row of rank - 1)
+  double *hs_dn, *hz_dn;   // row below the band (first row of rank + 1)
+  double *peer_up_hs, *peer_up_hz;  // rank - 1's hs_dn / hz_dn
+  double *peer_dn_hs, *peer_dn_hz;  // rank + 1's hs_up / hz_up
 };
 
 // Reduced operator row (nonorthogonal_mi.c:394-409), evaluated in the
 // reference's order.  s holds this band's rows; pole is the pole value.
 __device__ __forceinline__ double apply_row(const double *s, const Band &b,
-                                            const Row &rw, int np, int R,
-                                            int l, int j, int p, double pole) {
+                                            const Row &rw, int np, int l, int j,
+                                            int p, double pole) {
   const double c = s[p];
   const double sm = j == 0 ? s[p + np - 1] : s[p - 1];
   const double sp = j == np - 1 ? s[p - np + 1] : s[p + 1];
   double lv, uv;
   if (l > 0) lv = s[p - np];
-  else lv = b.ra == 0 ? pole : b.up[b.up_last + j];
+  else lv = b.top ? pole : b.hs_up[j];
   if (l < b.nrow - 1) uv = s[p + np];
-  else uv = b.ra + b.nrow == R ? 0.0 : b.dn[j];
+  else uv = b.bottom ? 0.0 : b.hs_dn[j];
   return rw.w * (rw.lo * (c - lv) + rw.up * (c - uv) +
                  rw.lon * (2.0 * c - sm - sp));
+}
+
+// Sets s[p] of an owned point and pushes it to the neighbour whose halo
+// row holds it.
+__device__ __forceinline__ void set_s(double *s, const Band &b, int l, int j, int p,
+                                      double v) {
+  s[p] = v;
+  if (l == 0 && !b.top) b.peer_up_hs[j] = v;
+  if (l == b.nrow - 1 && !b.bottom) b.peer_dn_hs[j] = v;
 }
 
 // Walks the points p = t, t + kThreads, ... of a band of nrow rows of np
@@ -176,32 +194,33 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int t = threadIdx.x;
 
   extern __shared__ __align__(16) double dyn[];
-  __shared__ double wbuf[kWarps * kSlotWidth];
-  __shared__ double slots[kSlots * kSlotWidth];
+  __shared__ double wbuf[32 * kSlotWidth];
+  __shared__ double slots[kSlots * kMaxCluster * kSlotWidth];
   __shared__ double pole_s;
 
   Band b;
   b.ra = (int)((long long)rank * R / csize);
   const int rb = (int)((long long)(rank + 1) * R / csize);
   b.nrow = rb - b.ra;
+  b.top = rank == 0;
+  b.bottom = rank == csize - 1;
   const int P = b.nrow * np;
   const size_t stride = (size_t)((R + csize - 1) / csize) * np;
-  double *s = dyn;               // search direction (read by neighbours)
+  double *s = dyn;               // search direction
   double *xs = dyn + stride;     // solution
   double *rs = dyn + 2 * stride; // residual
   double *as = dyn + 3 * stride; // A s
-  Row *rt = reinterpret_cast<Row *>(dyn + 4 * stride);
-  b.up = nullptr;
-  b.dn = nullptr;
-  b.up_last = 0;
-  if (rank > 0) {
-    b.up = cl.map_shared_rank(s, rank - 1);
-    const int ra_up = (int)((long long)(rank - 1) * R / csize);
-    b.up_last = (b.ra - ra_up - 1) * np;
-  }
-  if (rank + 1 < csize) b.dn = cl.map_shared_rank(s, rank + 1);
+  b.hs_up = dyn + 4 * stride;
+  b.hz_up = b.hs_up + np;
+  b.hs_dn = b.hz_up + np;
+  b.hz_dn = b.hs_dn + np;
+  Row *rt = reinterpret_cast<Row *>(b.hz_dn + np);
+  b.peer_up_hs = b.top ? nullptr : cl.map_shared_rank(b.hs_dn, rank - 1);
+  b.peer_up_hz = b.top ? nullptr : cl.map_shared_rank(b.hz_dn, rank - 1);
+  b.peer_dn_hs = b.bottom ? nullptr : cl.map_shared_rank(b.hs_up, rank + 1);
+  b.peer_dn_hz = b.bottom ? nullptr : cl.map_shared_rank(b.hz_up, rank + 1);
   for (int l = t; l < b.nrow; l += kThreads) rt[l] = S.rows[b.ra + l];
-  const bool lead = rank == 0;
+  const bool lead = b.top;
   const double dnp = (double)np;
   const double ps = dnp * S.pe;  // pole diagonal and pole residual scale
   const Walk W(t, np);
@@ -223,7 +242,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const double v = S.pot[(size_t)(b.ra + l + 1) * np + j];
     const double xv = isfinite(v) ? v : 0.0;
     xs[p] = xv;
-    s[p] = xv;
+    set_s(s, b, l, j, p, xv);
   }
   if (lead && t == 0) pole_s = x0;
   cl.sync();
@@ -238,7 +257,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const double f = S.fac[(size_t)(b.ra + l + 1) * np + j];
       const double u = S.neg_r2 * f * rw.inc;
       const double rhs = rw.w * u + rw.extra;
-      const double ax = apply_row(s, b, rw, np, R, l, j, p, pole);
+      const double ax = apply_row(s, b, rw, np, l, j, p, pole);
       const double r = rhs - ax;
       rs[p] = r;
       const double q = r * rw.rw;
@@ -258,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     out[0] = v[0];
     out[1] = v[1];
     out[2] = v[2];
-    cluster_sum<3>(cl, out, slots, ctr, csize);
+    cluster_sum<3>(cl, out, slots, ctr, rank, csize);
   };
 
   // z = M^-1 r, s = z, rho = r . z
@@ -267,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     GCS_MI_FOR_POINTS(W, P, np) {
       const double r = rs[p];
       const double z = r * rt[l].rdg;
-      s[p] = z;
+      set_s(s, b, l, j, p, z);
       v[0] += r * z;
     }
     block_sum<1>(v, wbuf);
@@ -276,7 +295,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       v[0] += r0 * z0;
       if (t == 0) pole_s = z0;
     }
-    cluster_sum<1>(cl, v, slots, ctr, csize);
+    cluster_sum<1>(cl, v, slots, ctr, rank, csize);
     return v[0];
   };
 
@@ -299,7 +318,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       double v[2] = {0.0, 0.0};  // s.As, first-ring sum of s
       const double pole = lead ? pole_s : 0.0;
       GCS_MI_FOR_POINTS(W, P, np) {
-        const double a = apply_row(s, b, rt[l], np, R, l, j, p, pole);
+        const double a = apply_row(s, b, rt[l], np, l, j, p, pole);
         as[p] = a;
         v[0] += s[p] * a;
         if (b.ra + l == 0) v[1] += s[p];
@@ -311,10 +330,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         As0 = S.pe * (dnp * pole - v[1]);
         den[0] += pole * As0;
       }
-      cluster_sum<1>(cl, den, slots, ctr, csize);
+      cluster_sum<1>(cl, den, slots, ctr, rank, csize);
       if (!isfinite(den[0]) || den[0] <= DBL_MIN) break;
       const double alpha = rho / den[0];
-      // x += alpha s, r -= alpha A s; residual norm and r . M^-1 r
+      // x += alpha s, r -= alpha A s; residual norm and r . M^-1 r.  The
+      // band's edge rows of z go to the neighbours, which then advance
+      // their halo copies of s themselves.
       double w2[2] = {0.0, 0.0};
       GCS_MI_FOR_POINTS(W, P, np) {
         const Row &rw = rt[l];
@@ -322,8 +343,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         const double r = rs[p] - alpha * as[p];
         rs[p] = r;
         const double q = r * rw.rw;
+        const double z = r * rw.rdg;
         w2[0] += q * q;
-        w2[1] += r * (r * rw.rdg);
+        w2[1] += r * z;
+        if (l == 0 && !b.top) b.peer_up_hz[j] = z;
+        if (l == b.nrow - 1 && !b.bottom) b.peer_dn_hz[j] = z;
       }
       block_sum<2>(w2, wbuf);
       if (lead) {
@@ -333,12 +357,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         w2[0] += dnp * pr * pr;
         w2[1] += r0 * (r0 / ps);
       }
-      cluster_sum<2>(cl, w2, slots, ctr, csize);
+      cluster_sum<2>(cl, w2, slots, ctr, rank, csize);
       final_res = sqrt(fmax(0.0, w2[0]));
       iters = it;
       if (final_res <= target || it % kTruePeriod == 0) {
         // Verify with the true residual (nonorthogonal_mi.c:562-582).
-        GCS_MI_FOR_POINTS(W, P, np) { s[p] = xs[p]; }
+        GCS_MI_FOR_POINTS(W, P, np) { set_s(s, b, l, j, p, xs[p]); }
         if (lead && t == 0) pole_s = x0;
         cl.sync();
         true_residual(tr);
@@ -354,28 +378,289 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!isfinite(rho_new) || rho_new <= DBL_MIN) break;
       const double beta = rho_new / rho;
       GCS_MI_FOR_POINTS(W, P, np) { s[p] = rs[p] * rt[l].rdg + beta * s[p]; }
+      for (int j = t; j < np; j += kThreads) {
+        if (!b.top) b.hs_up[j] = b.hz_up[j] + beta * b.hs_up[j];
+        if (!b.bottom) b.hs_dn[j] = b.hz_dn[j] + beta * b.hs_dn[j];
+      }
       if (lead && t == 0) pole_s = r0 / ps + beta * pole;
       rho = rho_new;
-      cl.sync();
+      __syncthreads();
     }
   }
 
   if (bad) {
     if (lead && t == 0) *S.status = 2;
-    cl.sync();  // no CTA leaves while a peer may still read its slots
+    cl.sync();  // no CTA leaves while a peer may still write its memory
     return;
   }
   // Expand the reduced solution (nonorthogonal_mi.c:595-605).
   GCS_MI_FOR_POINTS(W, P, np) { S.pot[(size_t)(b.ra + l + 1) * np + j] = xs[p]; }
   if (lead)
     for (int j = t; j < np; j += kThreads) S.pot[j] = x0;
-  if (rb == R)
+  if (b.bottom)
     for (int j = t; j < np; j += kThreads) S.pot[(size_t)(S.nt - 1) * np + j] = S.low;
   if (lead && t == 0) {
     *S.stats = gamera_mi_solver_stats{iters, initial, final_res, conv};
     *S.status = conv ? 0 : 1;
   }
-  cl.sync();  // no CTA leaves while a peer may still read its shared memory
+  cl.sync();  // no CTA leaves while a peer may still write its memory
+}
+
+// ------------------------------------------------------- column kernel
+// The same solve with one thread per longitude column of the band: thread
+// j keeps the band's column of s, x, r and A s in registers (MR rows at
+// most), takes the vertical stencil neighbours from its own registers and
+// only the longitude neighbours from shared memory.  Used when the grid fits
+// (np <= col_threads(MR), band rows <= MR); k_pcg serves the rest.
+
+__host__ __device__ constexpr int col_threads(int mr) {
+  return mr <= 4 ? 512 : (mr <= 12 ? 384 : 256);
+}
+
+template <int MR>
+__global__ void __launch_bounds__(col_threads(MR), 1)
+    k_pcg_col(const System *systems, int csize) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const System &S = systems[blockIdx.x / csize];
+  const int np = S.np, R = S.nt - 2;
+  const int j = threadIdx.x;
+  const bool on = j < np;
+  const int jm = j == 0 ? np - 1 : j - 1;
+  const int jp = j + 1 >= np ? 0 : j + 1;
+
+  extern __shared__ __align__(16) double dyn[];
+  __shared__ double wbuf[32 * kSlotWidth];
+  __shared__ double slots[kSlots * kMaxCluster * kSlotWidth];
+  __shared__ double pole_s;
+
+  // halo rows: [0] s above, [np] z above, [2np] s below, [3np] z below
+  const int ra = (int)((long long)rank * R / csize);
+  const int nrow = (int)((long long)(rank + 1) * R / csize) - ra;
+  const bool top = rank == 0, bottom = rank == csize - 1;
+  double *ssm = dyn;                    // MR rows of s
+  double *halo = dyn + (size_t)MR * np;
+  Row *rt = reinterpret_cast<Row *>(halo + 4 * (size_t)np);
+  // the neighbours' halo rows that this band's edge rows feed
+  double *peer_up = top ? nullptr : cl.map_shared_rank(halo, rank - 1) + 2 * np + j;
+  double *peer_dn = bottom ? nullptr : cl.map_shared_rank(halo, rank + 1) + j;
+  for (int l = j; l < nrow; l += blockDim.x) rt[l] = S.rows[ra + l];
+  const bool lead = top;
+  const double dnp = (double)np;
+  const double ps = dnp * S.pe;
+  int ctr = 0;
+
+  double sv[MR], xv[MR], rv[MR], av[MR];
+
+  // s of row l := v, in registers, shared memory and the neighbours' halos
+  auto put_s = [&](int l, double v) {
+    sv[l] = v;
+    ssm[l * np + j] = v;
+    if (l == 0 && !top) peer_up[0] = v;
+    if (l == nrow - 1 && !bottom) peer_dn[0] = v;
+  };
+  // A s of row l from the registers of the column (nonorthogonal_mi.c:394-409)
+  auto stencil = [&](int l, const Row &rw, double pole) {
+    const double c = sv[l];
+    const double sm = ssm[l * np + jm];
+    const double sp = ssm[l * np + jp];
+    const double lv = l > 0 ? sv[l > 0 ? l - 1 : 0] : (top ? pole : halo[j]);
+    const double uv = l < nrow - 1 ? sv[l + 1 < MR ? l + 1 : MR - 1]
+                                   : (bottom ? 0.0 : halo[2 * np + j]);
+    return rw.w * (rw.lo * (c - lv) + rw.up * (c - uv) +
+                   rw.lon * (2.0 * c - sm - sp));
+  };
+
+  double x0 = 0.0, r0 = 0.0;
+  if (lead) {
+    double pm[1] = {0.0};
+    for (int q = j; q < np; q += blockDim.x) {
+      const double v = S.pot[q];
+      if (isfinite(v)) pm[0] += v / dnp;
+    }
+    block_sum<1>(pm, wbuf);
+    x0 = pm[0];
+  }
+#pragma unroll
+  for (int l = 0; l < MR; ++l) {
+    xv[l] = 0.0;
+    rv[l] = 0.0;
+    av[l] = 0.0;
+    sv[l] = 0.0;
+    if (l < nrow && on) {
+      const double v = S.pot[(size_t)(ra + l + 1) * np + j];
+      xv[l] = isfinite(v) ? v : 0.0;
+      put_s(l, xv[l]);
+    }
+  }
+  if (lead && j == 0) pole_s = x0;
+  cl.sync();
+
+  auto true_residual = [&](double (&out)[3]) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};  // norm^2, rhs^2, bad, ring
+    const double pole = lead ? pole_s : 0.0;
+#pragma unroll
+    for (int l = 0; l < MR; ++l) {
+      if (l < nrow && on) {
+        const Row rw = rt[l];
+        const double f = S.fac[(size_t)(ra + l + 1) * np + j];
+        const double u = S.neg_r2 * f * rw.inc;
+        const double rhs = rw.w * u + rw.extra;
+        rv[l] = rhs - stencil(l, rw, pole);
+        const double q = rv[l] * rw.rw;
+        v[0] += q * q;
+        v[1] += u * u;
+        v[2] += isfinite(f) ? 0.0 : 1.0;
+        if (l == 0 && top) v[3] += sv[0];
+      }
+    }
+    block_sum<4>(v, wbuf);
+    if (lead) {
+      const double ax0 = S.pe * (dnp * pole - v[3]);
+      r0 = 0.0 - ax0;
+      const double pr = r0 / ps;
+      v[0] += dnp * pr * pr;
+      v[1] += dnp * S.low * S.low;
+    }
+    out[0] = v[0];
+    out[1] = v[1];
+    out[2] = v[2];
+    cluster_sum<3>(cl, out, slots, ctr, rank, csize);
+  };
+
+  auto restart = [&]() -> double {
+    double v[1] = {0.0};
+#pragma unroll
+    for (int l = 0; l < MR; ++l) {
+      if (l < nrow && on) {
+        const double z = rv[l] * rt[l].rdg;
+        put_s(l, z);
+        v[0] += rv[l] * z;
+      }
+    }
+    block_sum<1>(v, wbuf);
+    if (lead) {
+      const double z0 = r0 / ps;
+      v[0] += r0 * z0;
+      if (j == 0) pole_s = z0;
+    }
+    cluster_sum<1>(cl, v, slots, ctr, rank, csize);
+    return v[0];
+  };
+
+  double tr[3];
+  true_residual(tr);
+  const double initial = sqrt(fmax(0.0, tr[0]));
+  const double target =
+      fmax(S.abs_tol, S.rel_tol * fmax(sqrt(fmax(0.0, tr[1])), 1.0));
+  const bool bad = tr[2] > 0.0;
+  double final_res = initial;
+  int iters = 0;
+  int conv = initial <= target;
+  const int max_iter = S.max_iter < kMaxIterations ? S.max_iter : kMaxIterations;
+
+  if (!bad && !conv) {
+    double rho = restart();
+    for (int it = 1; it <= max_iter; ++it) {
+      if (!isfinite(rho) || rho <= DBL_MIN) break;
+      double v[2] = {0.0, 0.0};  // s.As, first-ring sum of s
+      const double pole = lead ? pole_s : 0.0;
+#pragma unroll
+      for (int l = 0; l < MR; ++l) {
+        if (l < nrow && on) {
+          av[l] = stencil(l, rt[l], pole);
+          v[0] += sv[l] * av[l];
+          if (l == 0 && top) v[1] += sv[0];
+        }
+      }
+      block_sum<2>(v, wbuf);
+      double As0 = 0.0;
+      double den[1] = {v[0]};
+      if (lead) {
+        As0 = S.pe * (dnp * pole - v[1]);
+        den[0] += pole * As0;
+      }
+      cluster_sum<1>(cl, den, slots, ctr, rank, csize);
+      if (!isfinite(den[0]) || den[0] <= DBL_MIN) break;
+      const double alpha = rho / den[0];
+      double w2[2] = {0.0, 0.0};
+#pragma unroll
+      for (int l = 0; l < MR; ++l) {
+        if (l < nrow && on) {
+          const Row &rw = rt[l];
+          xv[l] += alpha * sv[l];
+          rv[l] -= alpha * av[l];
+          const double q = rv[l] * rw.rw;
+          const double z = rv[l] * rw.rdg;
+          w2[0] += q * q;
+          w2[1] += rv[l] * z;
+          if (l == 0 && !top) peer_up[np] = z;
+          if (l == nrow - 1 && !bottom) peer_dn[np] = z;
+        }
+      }
+      block_sum<2>(w2, wbuf);
+      if (lead) {
+        x0 += alpha * pole;
+        r0 -= alpha * As0;
+        const double pr = r0 / ps;
+        w2[0] += dnp * pr * pr;
+        w2[1] += r0 * (r0 / ps);
+      }
+      cluster_sum<2>(cl, w2, slots, ctr, rank, csize);
+      final_res = sqrt(fmax(0.0, w2[0]));
+      iters = it;
+      if (final_res <= target || it % kTruePeriod == 0) {
+#pragma unroll
+        for (int l = 0; l < MR; ++l)
+          if (l < nrow && on) put_s(l, xv[l]);
+        if (lead && j == 0) pole_s = x0;
+        cl.sync();
+        true_residual(tr);
+        final_res = sqrt(fmax(0.0, tr[0]));
+        if (final_res <= target) {
+          conv = 1;
+          break;
+        }
+        rho = restart();
+        continue;
+      }
+      const double rho_new = w2[1];
+      if (!isfinite(rho_new) || rho_new <= DBL_MIN) break;
+      const double beta = rho_new / rho;
+#pragma unroll
+      for (int l = 0; l < MR; ++l) {
+        if (l < nrow && on) {
+          sv[l] = rv[l] * rt[l].rdg + beta * sv[l];
+          ssm[l * np + j] = sv[l];
+        }
+      }
+      if (on) {
+        if (!top) halo[j] = halo[np + j] + beta * halo[j];
+        if (!bottom) halo[2 * np + j] = halo[3 * np + j] + beta * halo[2 * np + j];
+      }
+      if (lead && j == 0) pole_s = r0 / ps + beta * pole;
+      rho = rho_new;
+      __syncthreads();
+    }
+  }
+
+  if (bad) {
+    if (lead && j == 0) *S.status = 2;
+    cl.sync();  // no CTA leaves while a peer may still write its memory
+    return;
+  }
+#pragma unroll
+  for (int l = 0; l < MR; ++l)
+    if (l < nrow && on) S.pot[(size_t)(ra + l + 1) * np + j] = xv[l];
+  if (lead)
+    for (int q = j; q < np; q += blockDim.x) S.pot[q] = x0;
+  if (bottom)
+    for (int q = j; q < np; q += blockDim.x) S.pot[(size_t)(S.nt - 1) * np + q] = S.low;
+  if (lead && j == 0) {
+    *S.stats = gamera_mi_solver_stats{iters, initial, final_res, conv};
+    *S.status = conv ? 0 : 1;
+  }
+  cl.sync();  // no CTA leaves while a peer may still write its memory
 }
 
 // ---------------------------------------------------------------- apply
@@ -559,24 +844,36 @@ std::vector<TensorRow> build_tensor_rows(const gamera_mi_solver_config *c) {
   return rows;
 }
 
-cudaError_t configure(int csize, size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+using PcgKernel = void (*)(const System *, int);
+
+// One launch shape of the solve: kernel, cluster size, threads per CTA and
+// dynamic shared memory.
+struct Shape {
+  PcgKernel kernel = nullptr;
+  int csize = 0, threads = 0, rows = 0;
+  size_t smem = 0;
+};
+
+cudaError_t configure(const Shape &sh) {
+  cudaError_t e = cudaFuncSetAttribute(sh.kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sh.smem);
   if (e != cudaSuccess) return e;
-  if (csize > kPortableCluster)
-    e = cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (sh.csize > kPortableCluster)
+    e = cudaFuncSetAttribute(sh.kernel, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                             1);
   return e;
 }
 
-cudaLaunchConfig_t launch_config(int csize, int count, size_t smem, cudaStream_t stream,
+cudaLaunchConfig_t launch_config(const Shape &sh, int count, cudaStream_t stream,
                                  cudaLaunchAttribute *attr) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(csize * count));
-  cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = smem;
+  cfg.gridDim = dim3((unsigned)(sh.csize * count));
+  cfg.blockDim = dim3((unsigned)sh.threads);
+  cfg.dynamicSmemBytes = sh.smem;
   cfg.stream = stream;
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)csize;
+  attr[0].val.clusterDim.x = (unsigned)sh.csize;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
@@ -584,24 +881,41 @@ cudaLaunchConfig_t launch_config(int csize, int count, size_t smem, cudaStream_t
   return cfg;
 }
 
-int max_clusters(int csize, size_t smem) {
-  if (configure(csize, smem) != cudaSuccess) {
+bool launchable(const Shape &sh) {
+  if (sh.smem > 200 * 1024 || configure(sh) != cudaSuccess) {
     cudaGetLastError();
-    return 0;
+    return false;
   }
   cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = launch_config(csize, 1, smem, nullptr, attr);
+  cudaLaunchConfig_t cfg = launch_config(sh, 1, nullptr, attr);
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k_pcg, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, sh.kernel, &cfg) != cudaSuccess) {
     cudaGetLastError();
-    return 0;
+    return false;
   }
-  return n;
+  return n >= 1;
 }
 
-// Shared memory of a band of `rows` rows: four vectors plus the row table.
+// Column kernel: MR rows of s plus four halo rows, and the row table.
+size_t col_smem(int mr, int np) {
+  return ((size_t)mr * np + 4 * (size_t)np) * sizeof(double) + (size_t)mr * sizeof(Row);
+}
+
+PcgKernel col_kernel(int mr) {
+  switch (mr) {
+    case 4: return k_pcg_col<4>;
+    case 8: return k_pcg_col<8>;
+    case 12: return k_pcg_col<12>;
+    case 16: return k_pcg_col<16>;
+    default: return nullptr;
+  }
+}
+
+// Shared memory of a band of `rows` rows: four vectors, four halo rows and
+// the row table.
 size_t band_smem(int rows, int np) {
-  return 4 * (size_t)rows * np * sizeof(double) + (size_t)rows * sizeof(Row);
+  return (4 * (size_t)rows * np + 4 * (size_t)np) * sizeof(double) +
+         (size_t)rows * sizeof(Row);
 }
 
 constexpr size_t kMaxSmem = 200 * 1024;
@@ -614,8 +928,7 @@ using namespace gcs::mi;
 struct gcs_mi_plan {
   int count = 0;
   int np = 0, nt = 0;
-  int csize = 0;
-  size_t smem = 0;
+  Shape shape;
   std::vector<gamera_mi_solver_config> configs;
   Row *d_rows = nullptr;          // count * (nt - 2)
   System *d_sys = nullptr;        // count
@@ -652,21 +965,43 @@ bool cuda_ok(cudaError_t e, const char *what) {
 
 // Cluster size: about 2048 unknowns per CTA, at most 16 CTAs (8 where the
 // device cannot co-schedule 16), every CTA owning at least one row.
-int choose_cluster(gcs_mi_plan *p) {
-  const int R = p->nt - 2;
-  const long long points = (long long)p->np * R;
+// Launch shape: the column kernel with the smallest band (most CTAs, at
+// most 16) whose rows fit its registers; otherwise the shared-memory kernel
+// with about 2048 unknowns per CTA (8 CTAs at most where the device cannot
+// co-schedule 16).
+int choose_shape(gcs_mi_plan *p) {
+  const int R = p->nt - 2, np = p->np;
+  const int threads = (np + 31) / 32 * 32;
+  for (int mr : {4, 8, 12, 16}) {
+    Shape sh;
+    sh.kernel = col_kernel(mr);
+    sh.csize = (R + mr - 1) / mr;
+    sh.threads = threads;
+    sh.rows = mr;
+    sh.smem = col_smem(mr, np);
+    if (threads > col_threads(mr) || sh.csize > kMaxCluster) continue;
+    if (launchable(sh)) {
+      p->shape = sh;
+      return 0;
+    }
+  }
+  const long long points = (long long)np * R;
   int want = (int)((points + 2047) / 2048);
   if (want < 1) want = 1;
   for (int limit : {kMaxCluster, kPortableCluster}) {
     const int top = limit < R ? limit : R;
     int csize = want < top ? want : top;
     for (; csize <= top; ++csize)
-      if (band_smem((R + csize - 1) / csize, p->np) <= kMaxSmem) break;
+      if (band_smem((R + csize - 1) / csize, np) <= kMaxSmem) break;
     if (csize > top) continue;
-    const size_t smem = band_smem((R + csize - 1) / csize, p->np);
-    if (max_clusters(csize, smem) >= 1) {
-      p->csize = csize;
-      p->smem = smem;
+    Shape sh;
+    sh.kernel = k_pcg;
+    sh.csize = csize;
+    sh.threads = kThreads;
+    sh.rows = (R + csize - 1) / csize;
+    sh.smem = band_smem(sh.rows, np);
+    if (launchable(sh)) {
+      p->shape = sh;
       return 0;
     }
   }
@@ -699,7 +1034,7 @@ gcs_mi_plan *plan_create(const gamera_mi_solver_config *configs, int count) {
   p->np = (int)configs[0].longitude_count;
   p->nt = (int)configs[0].colatitude_count;
   p->configs.assign(configs, configs + count);
-  if (choose_cluster(p) != 0) {
+  if (choose_shape(p) != 0) {
     plan_free(p);
     return nullptr;
   }
@@ -772,9 +1107,9 @@ bool plan_bind(gcs_mi_plan *p, const double *fac, double *pot, cudaStream_t stre
 
 int plan_launch(gcs_mi_plan *p, cudaStream_t stream) {
   cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = launch_config(p->csize, p->count, p->smem, stream, attr);
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg, (const System *)p->d_sys,
-                                           p->csize);
+  cudaLaunchConfig_t cfg = launch_config(p->shape, p->count, stream, attr);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, p->shape.kernel,
+                                           (const System *)p->d_sys, p->shape.csize);
   p->stream = stream;
   return cuda_ok(e, "MI solve launch") ? 0 : -1;
 }
@@ -815,9 +1150,9 @@ void gcs_mi_plan_destroy(gcs_mi_plan *plan) {
 int gcs_mi_plan_info(const gcs_mi_plan *plan, int *cluster_ctas, int *threads_per_cta,
                      size_t *shared_bytes) {
   if (!plan) return -1;
-  if (cluster_ctas) *cluster_ctas = plan->csize;
-  if (threads_per_cta) *threads_per_cta = kThreads;
-  if (shared_bytes) *shared_bytes = plan->smem;
+  if (cluster_ctas) *cluster_ctas = plan->shape.csize;
+  if (threads_per_cta) *threads_per_cta = plan->shape.threads;
+  if (shared_bytes) *shared_bytes = plan->shape.smem;
   return 0;
 }
 

@@ -206,3 +206,25 @@ def test_invalid_config_rejected():
                 cases.mi_config(16, 9, rel_tol=0.0)):
         assert glib().gamera_mi_solve_constant_pedersen(
             C.byref(bad), ptr(case.fac), ptr(pot), C.byref(st)) == -1
+
+
+@pytest.mark.parametrize("npl,nt,threads", [(361, 181, 384), (192, 22, 192),
+                                            (600, 12, 512)])
+def test_launch_shapes(npl, nt, threads):
+    """Grids up to 384 longitudes run the column kernel (one thread per
+    longitude); wider ones the shared-memory kernel (512 threads).  Both
+    against the oracle."""
+    from gamera_cube_b200 import abi, cases
+    L = glib()
+    case = cases.mi_case(npl, nt, seed=13)
+    plan = C.c_void_p()
+    assert L.gcs_mi_plan_create(C.byref(case.config), 1, C.byref(plan)) == 0
+    thr = C.c_int()
+    L.gcs_mi_plan_info(plan, None, C.byref(thr), None)
+    L.gcs_mi_plan_destroy(plan)
+    assert thr.value == threads
+    rc, pot, st = gpu_solve(case.config, case.fac, case.potential)
+    assert rc == 0
+    ref = oracle_solve(case.config, case.fac, case.potential)
+    assert ref[0] == 0
+    check_solution(case.config, case.fac, pot, st, ref[1], ref[2].iterations)

@@ -101,11 +101,11 @@ def _load():
         "gcs_mi_plan_results": (C.c_int, [C.c_void_p, P(abi.MiSolverStats),
                                           P(C.c_int)]),
     }
-    for name, (res, args) in sig.items():
-        fn = getattr(lib, name)
-        fn.restype = res
-        fn.argtypes = args
-    return lib
+    sig.update(abi.mi_dipole_signatures())
+    sig["gcs_context_mi_dipole_create"] = (
+        C.c_int, [C.c_void_p, P(abi.EarthStartup), P(abi.MiDipoleConfig),
+                  P(C.c_void_p)])
+    return abi.bind(lib, sig)
 
 
 lib = _load()

@@ -182,3 +182,83 @@ def storage_arrays(storage):
             _view(storage.maxwell_face_flux[d], 3 * nf).reshape(fe + (3,))
         out["edge_emf%d" % d] = _view(storage.edge_emf[d], ne).reshape(ee)
     return out
+
+
+class Dipole(C.Structure):
+    _fields_ = [("moment", Vec3)]
+
+
+class EarthStartup(C.Structure):
+    """cubedsphere/cubedsphere_earth_startup.h:10-24"""
+    _fields_ = [("inner_radius", C.c_double), ("density", C.c_double),
+                ("speed", C.c_double), ("mach", C.c_double), ("gamma", C.c_double),
+                ("ambient_density", C.c_double), ("ambient_pressure", C.c_double),
+                ("front_x", C.c_double), ("front_width", C.c_double),
+                ("cut_radius", C.c_double), ("cut_length", C.c_double),
+                ("imf", Vec3), ("dipole", Dipole)]
+
+
+class MiDipoleConfig(C.Structure):
+    """cubedsphere/cubedsphere_mi_dipole.h:16-28"""
+    _fields_ = [("azimuth_points", C.c_size_t), ("colatitude_points", C.c_size_t),
+                ("current_shell", C.c_size_t), ("ionosphere_radius_re", C.c_double),
+                ("pedersen_siemens", C.c_double), ("coupling_interval_s", C.c_double),
+                ("length_norm_m", C.c_double), ("speed_norm_m_s", C.c_double),
+                ("mass_density_norm_kg_m3", C.c_double),
+                ("maximum_iterations", C.c_int), ("relative_tolerance", C.c_double)]
+
+
+class MiAnalysisView(C.Structure):
+    """cubedsphere/cubedsphere_mi_dipole.h:32-39"""
+    _fields_ = [("azimuth_points", C.c_size_t), ("colatitude_points", C.c_size_t),
+                ("shell_j_cells", C.c_size_t), ("shell_k_cells", C.c_size_t),
+                ("maximum_colatitude_rad", C.c_double), ("epoch_s", C.c_double),
+                ("sample_radius_re", C.c_double), ("pedersen_siemens", C.c_double),
+                ("fac_parallel_a_m2", C.POINTER(C.c_double) * 2),
+                ("potential_v", C.POINTER(C.c_double) * 2)]
+
+
+def mi_dipole_signatures():
+    """ctypes signatures of the cubedsphere_mi_dipole.h entry points, shared
+    by this library and the reference build."""
+    P = C.POINTER
+    return {
+        "gamera_cs_mi_dipole_create": (C.c_int, [P(Grid), P(Storage),
+                                                 P(BackgroundField), P(EarthStartup),
+                                                 P(C.c_size_t), C.c_size_t,
+                                                 P(MiDipoleConfig), P(C.c_void_p)]),
+        "gamera_cs_mi_dipole_destroy": (None, [C.c_void_p]),
+        "gamera_cs_mi_dipole_create_potential_view": (
+            C.c_int, [P(EarthStartup), P(MiDipoleConfig), P(C.c_void_p)]),
+        "gamera_cs_mi_dipole_export_potential": (
+            C.c_int, [C.c_void_p, P(C.c_double), C.c_size_t, P(C.c_double),
+                      P(C.c_double)]),
+        "gamera_cs_mi_dipole_import_potential": (
+            C.c_int, [C.c_void_p, P(C.c_double), C.c_size_t, C.c_double, C.c_double]),
+        "gamera_cs_mi_dipole_maybe_update": (C.c_int, [C.c_void_p, C.c_double]),
+        "gamera_cs_mi_dipole_update_due": (C.c_int, [C.c_void_p, C.c_double]),
+        "gamera_cs_mi_dipole_ready": (C.c_int, [C.c_void_p]),
+        "gamera_cs_mi_dipole_potential": (C.c_int, [C.c_void_p, Vec3, P(C.c_double)]),
+        "gamera_cs_mi_dipole_apply_inner_emf": (C.c_int, [C.c_void_p, P(Storage),
+                                                          P(Grid), C.c_size_t]),
+        "gamera_cs_mi_dipole_ghost_velocity": (C.c_int, [C.c_void_p, Vec3, Vec3,
+                                                         P(Vec3)]),
+        "gamera_cs_mi_dipole_stats": (C.c_int, [C.c_void_p, P(C.c_double),
+                                                P(C.c_double), P(C.c_double),
+                                                P(C.c_double), P(MiSolverStats)]),
+        "gamera_cs_mi_dipole_analysis_view": (C.c_int, [C.c_void_p, P(MiAnalysisView)]),
+        "gamera_cs_mi_dipole_export_shell_current": (
+            C.c_int, [C.c_void_p, P(C.c_double), P(C.c_double), P(C.c_double),
+                      C.c_size_t]),
+        "gamera_cs_mi_dipole_write_csv": (C.c_int, [C.c_void_p, C.c_char_p]),
+        "gamera_cs_mi_dipole_write_shell_current_csv": (C.c_int, [C.c_void_p,
+                                                                  C.c_char_p]),
+    }
+
+
+def bind(lib, signatures):
+    for name, (res, args) in signatures.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib

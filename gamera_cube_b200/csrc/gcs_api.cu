@@ -401,6 +401,12 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
 
 namespace gcs {
 void set_api_error(const char *msg) { set_last(msg); }
+Context *context_for_grid(const gamera_no_grid grid[6], const size_t active[3],
+                          size_t ghost) {
+  gcs_context *ctx = context_for(grid, active, ghost);
+  return ctx ? &ctx->c : nullptr;
+}
+Context *context_of(gcs_context *ctx) { return ctx ? &ctx->c : nullptr; }
 }  // namespace gcs
 
 extern "C" {

@@ -716,6 +716,18 @@ int Context::init_case(int kind, size_t nr, size_t n, unsigned long long seed) {
     cc[f].resize(cells);
     GCS_BTRY(cudaMemcpyAsync(cc[f].data(), d_cen, cells * sizeof(gamera_no_vec3),
                              cudaMemcpyDeviceToHost, stream));
+    {
+      // innermost layers (layer-major, so a prefix of each array)
+      const int wl = D.g + 4 < D.E0 ? D.g + 4 : D.E0;
+      const size_t wc = (size_t)wl * D.E1 * D.E2;
+      const size_t wv = (size_t)(wl + 1) * (D.E1 + 1) * (D.E2 + 1);
+      win_layers = wl;
+      win_vertex[f].resize(wv);
+      GCS_BTRY(cudaMemcpyAsync(win_vertex[f].data(), vert, wv * sizeof(gamera_no_vec3),
+                               cudaMemcpyDeviceToHost, stream));
+      GCS_BTRY(cudaStreamSynchronize(stream));
+      win_centroid[f].assign(cc[f].begin(), cc[f].begin() + wc);
+    }
     for (int d = 0; d < 3; ++d) {
       const long long fc = (long long)(D.E0 + (d == 0)) * (D.E1 + (d == 1)) *
                            (D.E2 + (d == 2));

@@ -3,6 +3,8 @@
 // the caller's reference-layout host arrays and the device node layout.
 #pragma once
 
+#include <vector>
+
 #include <cstdio>
 
 #include "gamera_cs_types.h"
@@ -39,6 +41,12 @@ struct Context {
   int resident = 0;
   DevStatus host_status{};
   char error[256] = {0};
+  // Geometry of the innermost radial layers of a device-built case (cell
+  // centroids of layers [0, win_layers), vertices of [0, win_layers + 1)),
+  // kept for the ionosphere-coupling plans; empty for host-grid contexts.
+  int win_layers = 0;
+  std::vector<gamera_no_vec3> win_centroid[kFaces];
+  std::vector<gamera_no_vec3> win_vertex[kFaces];
   // per-stage timing (profiling mode)
   int profiling = 0;
   double stage_ms[16] = {0};

@@ -106,6 +106,63 @@ int gamera_mi_apply_conductance_tensor(const gamera_mi_solver_config *config,
                                        const double *pedersen, const double *hall,
                                        const double *potential_v, double *result);
 
+/* Magnetosphere-ionosphere coupling, cubedsphere/cubedsphere_mi_dipole.h.
+ * The FAC curl, polar sampling and both potential solves of an update run
+ * on the GPU holding the MHD state (the context of `grid`, shared with the
+ * step calls); the potential, FAC and solver stats are then held on the
+ * host, where the lookups below read them.  Potentials agree with the
+ * reference to the solver tolerance (see gamera_mi_solve_constant_pedersen). */
+typedef struct gamera_cs_mi_dipole gamera_cs_mi_dipole;
+/* cubedsphere_mi_dipole.h:40-41 */
+int gamera_cs_mi_dipole_analysis_view(const gamera_cs_mi_dipole *state,
+                                      gamera_cs_mi_analysis_view *view);
+/* cubedsphere_mi_dipole.h:44-46 */
+int gamera_cs_mi_dipole_export_shell_current(const gamera_cs_mi_dipole *state,
+                                             double *jparallel_a_m2, double *mlat_deg,
+                                             double *phi_deg, size_t count);
+/* cubedsphere_mi_dipole.h:51-57 */
+int gamera_cs_mi_dipole_create(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                               gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                               const gamera_no_background_field background[GAMERA_CS_FACE_COUNT],
+                               const gamera_cs_earth_startup *startup,
+                               const size_t active[3], size_t ghost,
+                               const gamera_cs_mi_dipole_config *config,
+                               gamera_cs_mi_dipole **result);
+/* cubedsphere_mi_dipole.h:58 */
+void gamera_cs_mi_dipole_destroy(gamera_cs_mi_dipole *state);
+/* cubedsphere_mi_dipole.h:62-65 */
+int gamera_cs_mi_dipole_create_potential_view(const gamera_cs_earth_startup *startup,
+                                              const gamera_cs_mi_dipole_config *config,
+                                              gamera_cs_mi_dipole **result);
+/* cubedsphere_mi_dipole.h:66-71 */
+int gamera_cs_mi_dipole_export_potential(const gamera_cs_mi_dipole *state, double *values,
+                                         size_t count, double *epoch_s,
+                                         double *next_update_s);
+int gamera_cs_mi_dipole_import_potential(gamera_cs_mi_dipole *state, const double *values,
+                                         size_t count, double epoch_s,
+                                         double next_update_s);
+/* cubedsphere_mi_dipole.h:75-80 */
+int gamera_cs_mi_dipole_maybe_update(gamera_cs_mi_dipole *state, double time_code);
+int gamera_cs_mi_dipole_update_due(const gamera_cs_mi_dipole *state, double time_code);
+int gamera_cs_mi_dipole_ready(const gamera_cs_mi_dipole *state);
+/* cubedsphere_mi_dipole.h:81-88 */
+int gamera_cs_mi_dipole_potential(const gamera_cs_mi_dipole *state, gamera_no_vec3 point,
+                                  double *potential_v);
+int gamera_cs_mi_dipole_apply_inner_emf(const gamera_cs_mi_dipole *state,
+                                        gamera_no_storage *storage,
+                                        const gamera_no_grid *grid, size_t wall_i);
+int gamera_cs_mi_dipole_ghost_velocity(const gamera_cs_mi_dipole *state,
+                                       gamera_no_vec3 point,
+                                       gamera_no_vec3 source_velocity,
+                                       gamera_no_vec3 *ghost_velocity);
+/* cubedsphere_mi_dipole.h:89-98 */
+int gamera_cs_mi_dipole_write_csv(const gamera_cs_mi_dipole *state, const char *prefix);
+int gamera_cs_mi_dipole_write_shell_current_csv(const gamera_cs_mi_dipole *state,
+                                                const char *prefix);
+int gamera_cs_mi_dipole_stats(const gamera_cs_mi_dipole *state, double *fac_min,
+                              double *fac_max, double *potential_min_v,
+                              double *potential_max_v, gamera_mi_solver_stats solve[2]);
+
 /* ---------------------------------------------------------------- Part 2 */
 
 typedef struct gcs_context gcs_context;
@@ -265,6 +322,13 @@ int gcs_context_set_resident(gcs_context *ctx, int on);
  * Grids up to about 100,000 unknowns per system are supported; larger ones
  * fail at plan creation.  maximum_iterations is clamped to 1,048,576. */
 typedef struct gcs_mi_plan gcs_mi_plan;
+/* Ionosphere coupling of a device-built case (gcs_context_create_case with
+ * a background): as gamera_cs_mi_dipole_create, with the state, geometry
+ * and B0 taken from the context; the shell must lie within the innermost
+ * four active layers (current_shell <= 2).  No reference counterpart. */
+int gcs_context_mi_dipole_create(gcs_context *ctx, const gamera_cs_earth_startup *startup,
+                                 const gamera_cs_mi_dipole_config *config,
+                                 gamera_cs_mi_dipole **result);
 int gcs_mi_plan_create(const gamera_mi_solver_config *configs, int count,
                        gcs_mi_plan **plan);
 void gcs_mi_plan_destroy(gcs_mi_plan *plan);

@@ -279,6 +279,53 @@ typedef struct {
   int converged;
 } gamera_mi_solver_stats;
 
+/* nonorthogonal/src/nonorthogonal/nonorthogonal_background.h:42-45 */
+typedef struct {
+  gamera_no_vec3 moment;
+} gamera_no_dipole;
+
+/* cubedsphere/cubedsphere_earth_startup.h:10-24 */
+typedef struct {
+  double inner_radius;
+  double density;
+  double speed;
+  double mach;
+  double gamma;
+  double ambient_density;
+  double ambient_pressure;
+  double front_x;
+  double front_width;
+  double cut_radius;
+  double cut_length;
+  gamera_no_vec3 imf;
+  gamera_no_dipole dipole;
+} gamera_cs_earth_startup;
+
+/* cubedsphere/cubedsphere_mi_dipole.h:16-28 */
+typedef struct gamera_cs_mi_dipole_config {
+  size_t azimuth_points;
+  size_t colatitude_points;
+  size_t current_shell; /* zero-based active radial cell */
+  double ionosphere_radius_re;
+  double pedersen_siemens;
+  double coupling_interval_s;
+  double length_norm_m;
+  double speed_norm_m_s;
+  double mass_density_norm_kg_m3;
+  int maximum_iterations;
+  double relative_tolerance;
+} gamera_cs_mi_dipole_config;
+
+/* cubedsphere/cubedsphere_mi_dipole.h:32-39 */
+typedef struct {
+  size_t azimuth_points, colatitude_points;
+  size_t shell_j_cells, shell_k_cells;
+  double maximum_colatitude_rad, epoch_s, sample_radius_re;
+  double pedersen_siemens;
+  const double *fac_parallel_a_m2[2];
+  const double *potential_v[2];
+} gamera_cs_mi_analysis_view;
+
 #ifdef __cplusplus
 }
 #endif

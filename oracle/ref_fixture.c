@@ -23,6 +23,7 @@
  */
 #include "cubedsphere_halo.h"
 #include "cubedsphere_interface.h"
+#include "cubedsphere_mi_dipole.h"
 #include "cubedsphere_step.h"
 #include "nonorthogonal_background.h"
 #include "nonorthogonal_initialization.h"
@@ -329,4 +330,38 @@ int fx_copy_storage(fx_case *dst, const fx_case *src) {
     }
   }
   return 0;
+}
+
+/* Ionosphere coupling on a fixture case.  fx_set_mi_field puts the analytic
+ * residual field of the reference MI shell test
+ * (cubedsphere/tests/test_cubedsphere_mi_shell.c:54-66) on every active cell
+ * of both time levels; fx_mi_create builds the reference coupling on the
+ * case through gamera_cs_mi_dipole_create. */
+int fx_set_mi_field(fx_case *c) {
+  for (int f = 0; f < GAMERA_CS_FACE_COUNT; ++f) {
+    const size_t *e = c->grid[f].cell_extent;
+    for (size_t i = c->ghost; i < c->ghost + c->active[0]; ++i)
+      for (size_t j = c->ghost; j < c->ghost + c->active[1]; ++j)
+        for (size_t k = c->ghost; k < c->ghost + c->active[2]; ++k) {
+          const size_t cell = gamera_no_index3(e, i, j, k);
+          const gamera_no_vec3 p = c->grid[f].cell[cell].centroid;
+          const double r2 = p.value[0] * p.value[0] + p.value[1] * p.value[1] +
+                            p.value[2] * p.value[2];
+          const gamera_no_vec3 b = {{0.03 * p.value[1] / r2, -0.02 * p.value[0] / r2,
+                                     0.01 * p.value[0] * p.value[2] / r2}};
+          c->storage[f].cell_magnetic[cell] = b;
+          c->storage[f].old_cell_magnetic[cell] = b;
+        }
+  }
+  return 0;
+}
+
+gamera_cs_mi_dipole *fx_mi_create(fx_case *c, const gamera_cs_earth_startup *startup,
+                                  const gamera_cs_mi_dipole_config *config) {
+  gamera_cs_mi_dipole *mi = NULL;
+  if (!c->use_background ||
+      gamera_cs_mi_dipole_create(c->grid, c->storage, c->background, startup,
+                                 c->active, c->ghost, config, &mi) != 0)
+    return NULL;
+  return mi;
 }

@@ -97,6 +97,11 @@ def ref():
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
+        abi.bind(lib, abi.mi_dipole_signatures())
+        P = C.POINTER
+        abi.bind(lib, {"fx_set_mi_field": (C.c_int, [C.c_void_p]),
+                       "fx_mi_create": (C.c_void_p, [C.c_void_p, P(abi.EarthStartup),
+                                                     P(abi.MiDipoleConfig)])})
         _ref = _bind_common(lib)
     return _ref
 

@@ -88,7 +88,31 @@ def main():
                                                    ptr(case.hall), ptr(probe), ptr(res))
             out[key + "tensor/apply"] = res
         print(name, "constant it", int(out[key + "constant/stats"][0]))
+    coupling(lib, out)
     np.savez_compressed(os.path.join(HERE, "reference_mi.npz"), **out)
+
+
+def coupling(lib, out):
+    """The reference coupling (cubedsphere_mi_dipole.c) on the wind fixture
+    case with the analytic residual field of the reference MI shell test:
+    one update at t = 0 and every output the coupling tests compare."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    import mi_util
+    kind, nr, n, seed = mi_util.COUPLING_CASE
+    case = refbind.Case(refbind.FX_WIND, nr, n, seed)
+    assert lib.fx_set_mi_field(case.handle) == 0
+    cfg = mi_util.coupling_config()
+    startup = mi_util.coupling_startup()
+    mi = lib.fx_mi_create(case.handle, C.byref(startup), C.byref(cfg))
+    assert mi
+    assert lib.gamera_cs_mi_dipole_update_due(mi, 0.0) == 1
+    assert lib.gamera_cs_mi_dipole_maybe_update(mi, 0.0) == 1
+    assert lib.gamera_cs_mi_dipole_update_due(mi, 0.0) == 0
+    res = mi_util.coupling_outputs(lib, mi, case, cfg)
+    for k, v in res.items():
+        out["coupling/" + k] = v
+    print("coupling iterations", res["stats"][:2], "fac range", res["stats"][4:6])
+    lib.gamera_cs_mi_dipole_destroy(mi)
 
 
 if __name__ == "__main__":

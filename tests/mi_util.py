@@ -1,4 +1,4 @@
-"""Shared helpers of the ionosphere-solve tests."""
+"""Shared helpers of the ionosphere-solve and coupling tests."""
 import ctypes as C
 import os
 import sys
@@ -64,3 +64,136 @@ def true_residual(apply_fn, cfg, fac, pot):
     target = max(cfg.absolute_tolerance,
                  cfg.relative_tolerance * max(np.sqrt(rhs2), 1.0))
     return float(np.sqrt(norm2)), float(target)
+
+
+# ------------------------------------------------------------- coupling
+COUPLING_CASE = ("wind", 12, 10, 7)     # kind, radial, angular, seed
+
+
+def coupling_config(np_=192, nt=22, shell=1, max_iterations=4000):
+    """The reference Earth driver's MI configuration
+    (cubedsphere/tests/test_cubedsphere_dipole_background.c:512-518)."""
+    c = abi.MiDipoleConfig()
+    c.azimuth_points = np_
+    c.colatitude_points = nt
+    c.current_shell = shell
+    c.ionosphere_radius_re = 1.0
+    c.pedersen_siemens = 5.0
+    c.coupling_interval_s = 10.0
+    c.length_norm_m = 6371000.0
+    c.speed_norm_m_s = 100000.0
+    c.mass_density_norm_kg_m3 = 1.67262192369e-21
+    c.maximum_iterations = max_iterations
+    c.relative_tolerance = 1e-8
+    return c
+
+
+def coupling_startup():
+    """Earth startup of the reference driver
+    (test_cubedsphere_dipole_background.c:282-294)."""
+    s = abi.EarthStartup()
+    s.inner_radius = 2.5
+    s.density = 5.0
+    s.speed = 4.0
+    s.mach = 10.0
+    s.gamma = 5.0 / 3.0
+    s.ambient_density = 1.0
+    s.ambient_pressure = 0.001
+    s.front_x = -30.0
+    s.front_width = 1.5
+    s.cut_radius = 16.0
+    s.cut_length = 8.0
+    s.dipole.moment.value[2] = -6761.730688424097
+    return s
+
+
+def cell_centroids(grid_face):
+    n = 1
+    for a in range(3):
+        n *= grid_face.cell_extent[a]
+    cells = np.ctypeslib.as_array(grid_face.cell, shape=(n,))
+    return np.ascontiguousarray(cells["centroid"]["value"], dtype=np.float64)
+
+
+def set_mi_field(case):
+    """Analytic residual B of the reference MI shell test
+    (cubedsphere/tests/test_cubedsphere_mi_shell.c:54-66) on every active
+    cell of both time levels, evaluated in the same operation order."""
+    g = case.ghost
+    act = [case.active[a] for a in range(3)]
+    for f in range(6):
+        e = [case.grid[f].cell_extent[a] for a in range(3)]
+        cen = cell_centroids(case.grid[f]).reshape(e[0], e[1], e[2], 3)
+        arr = case.arrays(f)
+        sl = (slice(g, g + act[0]), slice(g, g + act[1]), slice(g, g + act[2]))
+        p = cen[sl]
+        x, y, z = p[..., 0], p[..., 1], p[..., 2]
+        r2 = x * x + y * y + z * z
+        b = np.stack([0.03 * y / r2, -0.02 * x / r2, 0.01 * x * z / r2], axis=-1)
+        for name in ("cell_magnetic", "old_cell_magnetic"):
+            arr[name].reshape(e[0], e[1], e[2], 3)[sl] = b
+
+
+def probe_points(seed=3, count=40):
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal((count, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    return d * rng.uniform(1.2, 3.0, size=(count, 1))
+
+
+def coupling_outputs(lib, mi, case, cfg):
+    """Everything the coupling tests compare, from library `lib` (this
+    library or the reference build) after an update of coupling `mi` on
+    `case`: polar FAC and potential, shell J_parallel, solver stats,
+    potential lookups and ghost velocities at seeded probe points, and the
+    wall EMF that apply_inner_emf writes on face 0."""
+    P = C.POINTER(C.c_double)
+    out = {}
+    per = cfg.azimuth_points * cfg.colatitude_points
+    pot = np.zeros(2 * per)
+    ep, nx = C.c_double(), C.c_double()
+    assert lib.gamera_cs_mi_dipole_export_potential(mi, pot.ctypes.data_as(P), 2 * per,
+                                                    C.byref(ep), C.byref(nx)) == 0
+    out["potential"] = pot
+    out["times"] = np.array([ep.value, nx.value])
+    view = abi.MiAnalysisView()
+    assert lib.gamera_cs_mi_dipole_analysis_view(mi, C.byref(view)) == 0
+    out["fac"] = np.concatenate([np.ctypeslib.as_array(view.fac_parallel_a_m2[h],
+                                                       shape=(per,)).copy()
+                                 for h in range(2)])
+    out["view"] = np.array([view.maximum_colatitude_rad, view.sample_radius_re])
+    nsh = 6 * case.active[1] * case.active[2]
+    j, la, ph = np.zeros(nsh), np.zeros(nsh), np.zeros(nsh)
+    assert lib.gamera_cs_mi_dipole_export_shell_current(
+        mi, j.ctypes.data_as(P), la.ctypes.data_as(P), ph.ctypes.data_as(P), nsh) == 0
+    out["shell_j"], out["shell_mlat"], out["shell_phi"] = j, la, ph
+    st = (abi.MiSolverStats * 2)()
+    mm = [C.c_double() for _ in range(4)]
+    assert lib.gamera_cs_mi_dipole_stats(mi, *[C.byref(v) for v in mm], st) == 0
+    out["stats"] = np.array([st[0].iterations, st[1].iterations, st[0].final_residual,
+                             st[1].final_residual] + [v.value for v in mm])
+    pts = probe_points()
+    look = np.zeros(len(pts))
+    ghost = np.zeros((len(pts), 3))
+    for q, p in enumerate(pts):
+        v = abi.Vec3()
+        for a in range(3):
+            v.value[a] = p[a]
+        val = C.c_double()
+        assert lib.gamera_cs_mi_dipole_potential(mi, v, C.byref(val)) == 0
+        look[q] = val.value
+        src = abi.Vec3()
+        src.value[0], src.value[1], src.value[2] = 0.3, -0.2, 0.1
+        gv = abi.Vec3()
+        assert lib.gamera_cs_mi_dipole_ghost_velocity(mi, v, src, C.byref(gv)) == 0
+        ghost[q] = [gv.value[a] for a in range(3)]
+    out["lookup"], out["ghost_velocity"] = look, ghost
+    arr = case.arrays(0)
+    for d in (1, 2):
+        arr["edge_emf%d" % d][...] = 0.0
+    assert lib.gamera_cs_mi_dipole_apply_inner_emf(mi, C.byref(case.storage[0]),
+                                                   C.byref(case.grid[0]),
+                                                   case.ghost) == 0
+    out["wall_emf"] = np.concatenate([arr["edge_emf%d" % d].ravel().copy()
+                                      for d in (1, 2)])
+    return out

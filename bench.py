@@ -8,9 +8,17 @@ background, seeded +-1 % density noise, CFL 0.3 with the reference Earth
 driver's dt rule; outflow radial ghosts.  Synthetic state built on the
 device; state arrays are several GB, far larger than L2.
 
+Every 10 steps (--mi-every) the timed run also makes one magnetosphere-
+ionosphere coupling update on the device: the field-aligned current on the
+FAC shell (Stokes curl of the residual B), its samples on two 192 x 22
+polar grids and both hemisphere potential solves.
+
 Metric: cell-updates/s (active cells x steps / device time), whole job
 over all ranks.  --gpus N runs N independent replicas (one per GPU, weak
-scaling: the step has no inter-GPU exchange).
+scaling: the step has no inter-GPU exchange).  The line also carries the
+standalone ionosphere solve ("mi": 181 x 361 polar cap per hemisphere,
+constant Pedersen, rel. residual 1e-8): ms per call on the device, end to
+end through the drop-in, and the reference's single-thread CPU solve.
 
 --impl reference times the reference's own CPU step (oracle/_ref, the
 unmodified reference library, all host threads) on a bounded sample of the
@@ -167,9 +175,37 @@ def run_gpu(args):
     lib.gcs_case_options(KIND_WIND, C.byref(opts), C.byref(ts))
     stream = torch.cuda.ExternalStream(lib.gcs_context_stream(ctx), device=device)
 
+    # ionosphere coupling of the step (the reference Earth driver's MI:
+    # 192 x 22 per hemisphere, FAC shell 1, 5 S), updated every
+    # args.mi_every steps inside the timed region
+    mi = None
+    if args.mi_every > 0:
+        from gamera_cube_b200 import cases
+        mi_cfg, mi_startup = cases.mi_dipole_config(), cases.earth_startup()
+        mi = C.c_void_p()
+        if lib.gcs_context_mi_dipole_create(ctx, C.byref(mi_startup), C.byref(mi_cfg),
+                                            C.byref(mi)) != 0:
+            raise RuntimeError(lib.gcs_last_error().decode())
+    mi_dt_code = 10.0 / 63.71          # coupling interval in code time
+    mi_clock = [0.0]
+
+    def run_steps(count):
+        # K graph-replayed steps with an MI update before every mi_every-th
+        done = 0
+        while done < count:
+            chunk = count - done
+            if mi is not None:
+                chunk = min(chunk, args.mi_every)
+                if lib.gamera_cs_mi_dipole_maybe_update(mi, mi_clock[0]) != 1:
+                    raise RuntimeError("MI update failed: " +
+                                       lib.gcs_last_error().decode())
+                mi_clock[0] += mi_dt_code
+            if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, chunk, 1):
+                raise RuntimeError("step run failed")
+            done += chunk
+
     # warm-up (also captures the CUDA graph of one step)
-    if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, args.warmup, 1):
-        raise RuntimeError("warm-up failed")
+    run_steps(args.warmup)
     if lib.gcs_context_sync(ctx) != 0:
         raise RuntimeError("warm-up step failed")
 
@@ -180,8 +216,7 @@ def run_gpu(args):
     torch.cuda.synchronize(device)
     with ClockSampler(local) as clocks:
         start.record(stream)
-        if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, args.steps, 1):
-            raise RuntimeError("timed run failed")
+        run_steps(args.steps)
         stop.record(stream)
         torch.cuda.synchronize(device)
     barrier(dist, device)
@@ -242,12 +277,13 @@ def run_gpu(args):
     barrier(dist, device)
     e2e_value = total_cells * e2e_steps / e2e_s
 
-    mi = run_mi(lib, torch, device, args.mi_solves) if args.mi_solves > 0 else None
+    mi_solo = run_mi(lib, torch, device, args.mi_solves) if args.mi_solves > 0 else None
 
     result = None
     if rank == 0:
         clk = clocks.summary()
         launches_per_step = 24
+        mi_updates = 0 if mi is None else -(-args.steps // args.mi_every)
         result = {
             "metric": METRIC,
             "value": value,
@@ -266,12 +302,18 @@ def run_gpu(args):
                        "faces": 6, "angular": n, "radial": nr,
                        "cells_per_gpu": cells, "ghost": 4,
                        "graph": "one CUDA graph per step, device-side dt",
+                       "mi_coupling": ("none" if mi is None else
+                                       "every %d steps: shell FAC curl + polar "
+                                       "sampling + 2 hemisphere PCG solves, "
+                                       "192 x 22 per hemisphere" % args.mi_every),
                        "l2": "state arrays larger than L2 (no flush needed)",
                        "parallelism": "replicas x%d" % world,
                        "setup_s": round(setup_s, 2)},
-            "gpu_launches": launches_per_step * args.steps,
-            "gpu_launches_note": "MHD step graph only; each MI solve is one "
-                                 "launch (timed separately under \"mi\")",
+            "gpu_launches": launches_per_step * args.steps + 5 * mi_updates,
+            "gpu_launches_note": "24 kernels per step graph + 5 per MI coupling "
+                                 "update (4 FAC kernels, 1 two-hemisphere "
+                                 "solve); the standalone solves under \"mi\" "
+                                 "are timed separately",
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": hs.bytes_state,
@@ -289,12 +331,14 @@ def run_gpu(args):
                          (ms_local / args.steps * 1e-3) / 1e9 / hbm},
             "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         }
-        if mi is not None:
-            result["mi"] = mi
+        if mi_solo is not None:
+            result["mi"] = mi_solo
         if args.cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(args)
-            if mi is not None:
+            if mi_solo is not None:
                 result["mi"]["cpu_baseline"] = mi_cpu_baseline()
+    if mi is not None:
+        lib.gamera_cs_mi_dipole_destroy(mi)
     lib.gcs_context_destroy(ctx)
     if dist is not None:
         dist.destroy_process_group()
@@ -507,6 +551,9 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=16)
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--mi-every", type=int, default=10,
+                    help="steps between ionosphere coupling updates in the "
+                         "timed MHD run (0: no coupling)")
     ap.add_argument("--mi-solves", type=int, default=10,
                     help="timed ionosphere solves (0 skips the MI measurement)")
     args = ap.parse_args()

@@ -15,6 +15,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import abi
 from .abi import MiSolverConfig
 
 NORTH = 1
@@ -81,3 +82,44 @@ def mi_case(longitudes: int = 361, colatitudes: int = 181, seed: int = 7,
     potential = np.zeros((nt, npl))
     return MiCase(cfg, np.ascontiguousarray(fac), np.ascontiguousarray(pedersen),
                   np.ascontiguousarray(hall), potential)
+
+
+def mi_dipole_config(azimuth=192, colatitude=22, shell=1, max_iterations=4000):
+    """The reference Earth driver's coupling configuration
+    (cubedsphere/tests/test_cubedsphere_dipole_background.c:512-518):
+    192 x 22 per hemisphere, FAC shell 1, R_I = 1 R_E, 5 S, 10 s cadence,
+    Earth normalisation (1 R_E, 100 km/s, 1 proton cm^-3), rel. tol. 1e-8."""
+    c = abi.MiDipoleConfig()
+    c.azimuth_points = azimuth
+    c.colatitude_points = colatitude
+    c.current_shell = shell
+    c.ionosphere_radius_re = 1.0
+    c.pedersen_siemens = 5.0
+    c.coupling_interval_s = 10.0
+    c.length_norm_m = 6371000.0
+    c.speed_norm_m_s = 100000.0
+    c.mass_density_norm_kg_m3 = 1.67262192369e-21
+    c.maximum_iterations = max_iterations
+    c.relative_tolerance = 1e-8
+    return c
+
+
+def earth_startup():
+    """Earth startup of the reference driver
+    (test_cubedsphere_dipole_background.c:282-294): inner radius 2.5 R_E,
+    n = 5, V = 4 (400 km/s), Mach 10, front at x = -30, dipole cut at
+    16 +- 8 R_E, moment (0, 0, -6761.73) (0.31 G equatorial surface field)."""
+    s = abi.EarthStartup()
+    s.inner_radius = 2.5
+    s.density = 5.0
+    s.speed = 4.0
+    s.mach = 10.0
+    s.gamma = 5.0 / 3.0
+    s.ambient_density = 1.0
+    s.ambient_pressure = 0.001
+    s.front_x = -30.0
+    s.front_width = 1.5
+    s.cut_radius = 16.0
+    s.cut_length = 8.0
+    s.dipole.moment.value[2] = -6761.730688424097
+    return s

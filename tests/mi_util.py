@@ -71,40 +71,11 @@ COUPLING_CASE = ("wind", 12, 10, 7)     # kind, radial, angular, seed
 
 
 def coupling_config(np_=192, nt=22, shell=1, max_iterations=4000):
-    """The reference Earth driver's MI configuration
-    (cubedsphere/tests/test_cubedsphere_dipole_background.c:512-518)."""
-    c = abi.MiDipoleConfig()
-    c.azimuth_points = np_
-    c.colatitude_points = nt
-    c.current_shell = shell
-    c.ionosphere_radius_re = 1.0
-    c.pedersen_siemens = 5.0
-    c.coupling_interval_s = 10.0
-    c.length_norm_m = 6371000.0
-    c.speed_norm_m_s = 100000.0
-    c.mass_density_norm_kg_m3 = 1.67262192369e-21
-    c.maximum_iterations = max_iterations
-    c.relative_tolerance = 1e-8
-    return c
+    return cases.mi_dipole_config(np_, nt, shell, max_iterations)
 
 
 def coupling_startup():
-    """Earth startup of the reference driver
-    (test_cubedsphere_dipole_background.c:282-294)."""
-    s = abi.EarthStartup()
-    s.inner_radius = 2.5
-    s.density = 5.0
-    s.speed = 4.0
-    s.mach = 10.0
-    s.gamma = 5.0 / 3.0
-    s.ambient_density = 1.0
-    s.ambient_pressure = 0.001
-    s.front_x = -30.0
-    s.front_width = 1.5
-    s.cut_radius = 16.0
-    s.cut_length = 8.0
-    s.dipole.moment.value[2] = -6761.730688424097
-    return s
+    return cases.earth_startup()
 
 
 def cell_centroids(grid_face):

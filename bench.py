@@ -556,11 +556,20 @@ def main():
                          "timed MHD run (0: no coupling)")
     ap.add_argument("--mi-solves", type=int, default=10,
                     help="timed ionosphere solves (0 skips the MI measurement)")
+    ap.add_argument("--only-mi", action="store_true",
+                    help="run only the standalone ionosphere solve measurement "
+                         "(prints its JSON object; for profiling)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.only_mi:
+        import torch
+        import gamera_cube_b200
+        torch.cuda.set_device(0)
+        print(json.dumps(run_mi(gamera_cube_b200.lib, torch, torch.device("cuda", 0),
+                                max(1, args.mi_solves))))
     else:
         run_gpu(args)
 

@@ -278,6 +278,7 @@ def run_gpu(args):
     e2e_value = total_cells * e2e_steps / e2e_s
 
     mi_solo = run_mi(lib, torch, device, args.mi_solves) if args.mi_solves > 0 else None
+    bulk = run_bulk(lib, torch, device, args, dist) if args.bulk else None
 
     result = None
     if rank == 0:
@@ -333,6 +334,8 @@ def run_gpu(args):
         }
         if mi_solo is not None:
             result["mi"] = mi_solo
+        if bulk is not None:
+            result["fp32_bulk"] = bulk
         if args.cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(args)
             if mi_solo is not None:
@@ -344,6 +347,51 @@ def run_gpu(args):
         dist.destroy_process_group()
     if result is not None:
         print(json.dumps(result))
+
+
+def run_bulk(lib, torch, device, args, dist):
+    """FP32-bulk variant: the same workload and timing as the main line,
+    and its error after 1000 steps against the FP64 path on the
+    6 x 32x32x48 wind case (same time levels, gamera_cube_b200.precision)."""
+    from gamera_cube_b200 import abi, precision
+    nr, n = args.nr, args.n
+    ctx = lib.gcs_context_create_case(KIND_WIND, nr, n, 1000)
+    if not ctx or lib.gcs_context_set_precision(ctx, 1) != 0:
+        raise RuntimeError(lib.gcs_last_error().decode())
+    split = lib.gcs_context_bulk_split(ctx)
+    opts, ts = abi.AdvanceOptions(), abi.TimestepOptions()
+    lib.gcs_case_options(KIND_WIND, C.byref(opts), C.byref(ts))
+    stream = torch.cuda.ExternalStream(lib.gcs_context_stream(ctx), device=device)
+    if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, args.warmup, 1) != 0:
+        raise RuntimeError("bulk warm-up failed")
+    lib.gcs_context_sync(ctx)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    start.record(stream)
+    if lib.gcs_context_run(ctx, C.byref(opts), C.byref(ts), 0.5, args.steps, 1) != 0:
+        raise RuntimeError("bulk run failed")
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    if lib.gcs_context_sync(ctx) != 0:
+        raise RuntimeError("a bulk step failed")
+    ms = max_over_ranks(start.elapsed_time(stop), dist, device)
+    lib.gcs_context_destroy(ctx)
+    cells = sum_over_ranks(float(6 * nr * n * n), dist, device)
+    err = precision.compare_bulk(lib, KIND_WIND, 48, 32, 1000)
+    worst = max(err[v]["linf"] for v in precision.VARIABLES)
+    return {"value": cells * args.steps / (ms * 1e-3), "unit": "cell-updates/s",
+            "ms_per_step": ms / args.steps, "fp64_radial_layers": split,
+            "radial_layers": nr + 8,
+            "error_after_1000_steps": {"workload": "6 x 32x32x48 wind + dipole",
+                                       "max_rel_linf": worst,
+                                       "per_variable": {v: err[v] for v in
+                                                        precision.VARIABLES},
+                                       "div_b_bulk": err["div_b_bulk"],
+                                       "div_b_fp64": err["div_b_fp64"]},
+            "note": "flux/face-velocity/EMF sweeps in FP32 outside the layers "
+                    "where |B0| > 8 (those stay FP64); state, face B, CT, "
+                    "predictor and recovery FP64"}
 
 
 MI_GRID = (361, 181)            # longitudes, colatitudes per hemisphere
@@ -556,6 +604,8 @@ def main():
                          "timed MHD run (0: no coupling)")
     ap.add_argument("--mi-solves", type=int, default=10,
                     help="timed ionosphere solves (0 skips the MI measurement)")
+    ap.add_argument("--no-bulk", dest="bulk", action="store_false",
+                    help="skip the FP32-bulk variant measurement")
     ap.add_argument("--only-mi", action="store_true",
                     help="run only the standalone ionosphere solve measurement "
                          "(prints its JSON object; for profiling)")

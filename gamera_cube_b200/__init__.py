@@ -13,12 +13,13 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBRARY_PATH = os.path.join(_HERE, "libgamera_cs_b200.so")
 
 
-def _load():
-    if not os.path.exists(LIBRARY_PATH):
+def _load(path=None):
+    path = path or LIBRARY_PATH
+    if not os.path.exists(path):
         raise ImportError(
             "libgamera_cs_b200.so is not built (run make -C gamera_cube_b200); "
             "the CUDA library is required, there is no CPU fallback")
-    lib = C.CDLL(LIBRARY_PATH, mode=os.RTLD_LOCAL | getattr(os, "RTLD_NOW", 2))
+    lib = C.CDLL(path, mode=os.RTLD_LOCAL | getattr(os, "RTLD_NOW", 2))
     P = C.POINTER
     c_sz3 = C.c_size_t * 3
     sig = {
@@ -101,6 +102,10 @@ def _load():
         "gcs_mi_plan_results": (C.c_int, [C.c_void_p, P(abi.MiSolverStats),
                                           P(C.c_int)]),
     }
+    sig["gcs_context_set_precision"] = (C.c_int, [C.c_void_p, C.c_int])
+    sig["gcs_context_precision"] = (C.c_int, [C.c_void_p])
+    sig["gcs_context_set_bulk_threshold"] = (C.c_int, [C.c_void_p, C.c_double])
+    sig["gcs_context_bulk_split"] = (C.c_int, [C.c_void_p])
     sig.update(abi.mi_dipole_signatures())
     sig["gcs_context_mi_dipole_create"] = (
         C.c_int, [C.c_void_p, P(abi.EarthStartup), P(abi.MiDipoleConfig),

@@ -221,6 +221,11 @@ bool device_failed(gcs::Context &C) {
 int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
              const Hooks *hk) {
   gcs::Context &C = ctx->c;
+  if (hk && C.X.bulk &&
+      (hk->radial || hk->options->fluid_flux_sync || hk->options->edge_emf_sync)) {
+    C.set_error("host callbacks need the FP64 path", "step");
+    return -1;
+  }
   const gcs::Ctx &X = C.X;
   cudaStream_t s = C.stream;
   Marker mk{ctx};
@@ -365,9 +370,12 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
             background[f].face_flux[d] == nullptr ||
             (O.u_mhd && background[f].edge_magnetic[d] == nullptr))
           return -1;
-    if (!C.background_matches(background) && C.upload_background(background) != 0)
-      return -1;
+    if (!C.background_matches(background)) {
+      if (C.upload_background(background) != 0) return -1;
+      C.bulk_bg_dirty = 1;
+    }
   }
+  if (C.X.bulk && C.bulk_bg_dirty && C.enable_bulk(1) != 0) return -1;
   if (!(C.resident && C.resident_storage == storage)) {
     if (C.upload_state(storage) != 0) return -1;
   }
@@ -642,7 +650,9 @@ const char *gcs_context_error(const gcs_context *ctx) {
 int gcs_context_upload_background(gcs_context *ctx,
                                   const gamera_no_background_field bg[6]) {
   if (!ctx || !bg) return -1;
-  return ctx->c.upload_background(bg);
+  ctx->c.bulk_bg_dirty = 1;
+  if (ctx->c.upload_background(bg) != 0) return -1;
+  return ctx->c.X.bulk ? ctx->c.enable_bulk(1) : 0;
 }
 
 int gcs_context_upload_state(gcs_context *ctx, const gamera_no_storage st[6]) {
@@ -724,6 +734,7 @@ int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
     unsigned long long key = 1469598103934665603ULL;
     const unsigned char *b = (const unsigned char *)&O;
     for (size_t q = 0; q < sizeof(O); ++q) key = (key ^ b[q]) * 1099511628211ULL;
+    key = (key ^ (unsigned long long)C.X.bulk) * 1099511628211ULL;
     if (!C.graph_exec || C.graph_key != key) {
       if (C.graph_exec) cudaGraphExecDestroy(C.graph_exec);
       C.graph_exec = nullptr;
@@ -870,6 +881,36 @@ int gcs_context_set_resident(gcs_context *ctx, int on) {
   ctx->c.resident = on;
   if (!on) ctx->c.resident_storage = nullptr;
   return 0;
+}
+
+int gcs_context_set_precision(gcs_context *ctx, int fp32_bulk) {
+  if (!ctx) {
+    set_last("null context");
+    return -1;
+  }
+  if (ctx->c.enable_bulk(fp32_bulk ? 1 : 0) != 0) {
+    set_last(ctx->c.error);
+    return -1;
+  }
+  return 0;
+}
+
+int gcs_context_precision(const gcs_context *ctx) { return ctx ? ctx->c.X.bulk : -1; }
+
+int gcs_context_set_bulk_threshold(gcs_context *ctx, double b0_threshold) {
+  if (!ctx || !std::isfinite(b0_threshold) || b0_threshold < 0.0) {
+    set_last("invalid threshold");
+    return -1;
+  }
+  if (ctx->c.set_bulk_split(b0_threshold) != 0) {
+    set_last(ctx->c.error);
+    return -1;
+  }
+  return 0;
+}
+
+int gcs_context_bulk_split(const gcs_context *ctx) {
+  return ctx ? ctx->c.X.bulk_split : -1;
 }
 
 }  // extern "C"

@@ -60,6 +60,14 @@ struct Context {
   int init_case(int kind, size_t nr, size_t n, unsigned long long seed);
   int allocate(const size_t active[3], size_t ghost);
   int allocate_background();
+  // FP32-bulk sweeps on (1) or off (0); the FP32 arrays are allocated and
+  // the metric and background converted on first use (gcs_setup.cu).
+  int enable_bulk(int on);
+  void *bulk_pool = nullptr;
+  size_t bulk_bytes = 0;
+  int bulk_bg_dirty = 0;   // background uploaded since its FP32 copies
+  double bulk_b0_threshold = 8.0;   // |B0| above which a layer stays FP64
+  int set_bulk_split(double b0_threshold);
   int derive();
   int build_plans(const HaloGeometry &geo);
   void release();

@@ -76,6 +76,22 @@ struct DevBg {
   double *eb0t1[3], *eb0t2[3];   // edge B0 . t1, B0 . t2 per edge family
 };
 
+// The arrays the predictor writes for the sweeps and the metric and
+// background the sweeps read, in the sweeps' compute type T, plus the sweep
+// outputs, which are FP64 in both paths.  Bulk<double> views the FP64
+// arrays of DevState/DevGeom/DevBg; Bulk<float> views separate FP32 copies
+// (FP32-bulk path) and the same FP64 outputs.
+template <typename T>
+struct Bulk {
+  T *Pr[5], *Bp[3], *BN[3], *W[3];
+  double *FV[3][3], *F[3][5], *M[3][3], *E[3];
+  const T *vol, *iv[3], *area[3];
+  const T *fn[3][3], *ft1[3][3], *ft2[3][3];
+  const T *elen[3], *et1[3][3], *et2[3][3], *en1[3][2], *en2[3][2], *einv[3];
+  const T *ca[3], *cb[3];
+  const T *fb0[3][3], *fb0n[3], *eb0t1[3], *eb0t2[3];
+};
+
 // Scalar parameters of one step.  dt and ratio live in device memory so a
 // captured CUDA graph can advance its own time step.
 struct StepParams {

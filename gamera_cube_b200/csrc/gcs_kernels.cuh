@@ -22,7 +22,19 @@ struct Ctx {
   int n_edge_groups = 0;
   StepParams *params = nullptr;   // device
   DevStatus *status = nullptr;    // device
+  int bulk = 0;                   // 1: FP32-bulk sweeps (B32)
+  int bulk_split = 0;             // radial layers [0, bulk_split) stay FP64
+  Bulk<float> B32{};
 };
+
+// Bulk<double> view of the FP64 arrays.
+Bulk<double> bulk64(const Ctx &X);
+
+// FP32-bulk sweeps over the radial range [i0, i1) (gcs_kernels_bulk.cu).
+void launch_flux_f32(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s);
+void launch_face_velocity_f32(const Ctx &X, const Opts &O, int i0, int i1,
+                              cudaStream_t s);
+void launch_edge_emf_f32(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s);
 
 void launch_seam_sync(const Ctx &X, int magnetic, cudaStream_t s);
 void launch_halo(const Ctx &X, cudaStream_t s);

@@ -11,15 +11,35 @@
 
 namespace gcs {
 
-struct Prim {
-  double rho, vx, vy, vz, p;
+// Precision-generic math used by the sweep operators: T = double is the
+// plain path (the reference's arithmetic), T = float the FP32-bulk path.
+template <typename T> struct Num;
+template <> struct Num<double> {
+  static constexpr double tiny = DBL_MIN;
+  __host__ __device__ static double erfc_(double x) { return ::erfc(x); }
+  __host__ __device__ static double exp_(double x) { return ::exp(x); }
+  __host__ __device__ static double sqrt_(double x) { return ::sqrt(x); }
+  __host__ __device__ static double hypot_(double a, double b) { return ::hypot(a, b); }
+};
+template <> struct Num<float> {
+  static constexpr float tiny = FLT_MIN;
+  __host__ __device__ static float erfc_(float x) { return ::erfcf(x); }
+  __host__ __device__ static float exp_(float x) { return ::expf(x); }
+  __host__ __device__ static float sqrt_(float x) { return ::sqrtf(x); }
+  __host__ __device__ static float hypot_(float a, float b) { return ::hypotf(a, b); }
 };
 
-__host__ __device__ inline double dot3(double ax, double ay, double az,
-                                       double bx, double by, double bz) {
+template <typename T>
+struct PrimT {
+  T rho, vx, vy, vz, p;
+};
+using Prim = PrimT<double>;
+
+template <typename T>
+__host__ __device__ inline T dot3(T ax, T ay, T az, T bx, T by, T bz) {
   // nonorthogonal_flux.c:9-15.  The sum starts at +0.0 as in the
   // reference, so a product of -0.0 yields the same +0.0 result.
-  double r = 0.0;
+  T r = T(0.0);
   r += ax * bx;
   r += ay * by;
   r += az * bz;
@@ -27,68 +47,72 @@ __host__ __device__ inline double dot3(double ax, double ay, double az,
 }
 
 // nonorthogonal_reconstruction.c:7-9, 19-26, 53-55
-__host__ __device__ inline double central8(const double s[8]) {
-  double r = 0.0;
-  r += (-3.0 / 840.0) * s[0];
-  r += (29.0 / 840.0) * s[1];
-  r += (-139.0 / 840.0) * s[2];
-  r += (533.0 / 840.0) * s[3];
-  r += (533.0 / 840.0) * s[4];
-  r += (-139.0 / 840.0) * s[5];
-  r += (29.0 / 840.0) * s[6];
-  r += (-3.0 / 840.0) * s[7];
+template <typename T>
+__host__ __device__ inline T central8(const T s[8]) {
+  T r = T(0.0);
+  r += T(-3.0 / 840.0) * s[0];
+  r += T(29.0 / 840.0) * s[1];
+  r += T(-139.0 / 840.0) * s[2];
+  r += T(533.0 / 840.0) * s[3];
+  r += T(533.0 / 840.0) * s[4];
+  r += T(-139.0 / 840.0) * s[5];
+  r += T(29.0 / 840.0) * s[6];
+  r += T(-3.0 / 840.0) * s[7];
   return r;
 }
 
 // nonorthogonal_reconstruction.c:11-13, 57-59
-__host__ __device__ inline double central6(const double s[8]) {
-  double r = 0.0;
-  r += (0.0) * s[0];
-  r += (1.0 / 60.0) * s[1];
-  r += (-8.0 / 60.0) * s[2];
-  r += (37.0 / 60.0) * s[3];
-  r += (37.0 / 60.0) * s[4];
-  r += (-8.0 / 60.0) * s[5];
-  r += (1.0 / 60.0) * s[6];
-  r += (0.0) * s[7];
+template <typename T>
+__host__ __device__ inline T central6(const T s[8]) {
+  T r = T(0.0);
+  r += T(0.0) * s[0];
+  r += T(1.0 / 60.0) * s[1];
+  r += T(-8.0 / 60.0) * s[2];
+  r += T(37.0 / 60.0) * s[3];
+  r += T(37.0 / 60.0) * s[4];
+  r += T(-8.0 / 60.0) * s[5];
+  r += T(1.0 / 60.0) * s[6];
+  r += T(0.0) * s[7];
   return r;
 }
 
 // nonorthogonal_reconstruction.c:15-17, 28-34
-__host__ __device__ inline double upwind7_left(const double w[8]) {
-  double r = 0.0;
-  r += (-3.0 / 420.0) * w[0];
-  r += (25.0 / 420.0) * w[1];
-  r += (-101.0 / 420.0) * w[2];
-  r += (319.0 / 420.0) * w[3];
-  r += (214.0 / 420.0) * w[4];
-  r += (-38.0 / 420.0) * w[5];
-  r += (4.0 / 420.0) * w[6];
+template <typename T>
+__host__ __device__ inline T upwind7_left(const T w[8]) {
+  T r = T(0.0);
+  r += T(-3.0 / 420.0) * w[0];
+  r += T(25.0 / 420.0) * w[1];
+  r += T(-101.0 / 420.0) * w[2];
+  r += T(319.0 / 420.0) * w[3];
+  r += T(214.0 / 420.0) * w[4];
+  r += T(-38.0 / 420.0) * w[5];
+  r += T(4.0 / 420.0) * w[6];
   return r;
 }
-__host__ __device__ inline double upwind7_right(const double w[8]) {
-  double r = 0.0;
-  r += (-3.0 / 420.0) * w[7];
-  r += (25.0 / 420.0) * w[6];
-  r += (-101.0 / 420.0) * w[5];
-  r += (319.0 / 420.0) * w[4];
-  r += (214.0 / 420.0) * w[3];
-  r += (-38.0 / 420.0) * w[2];
-  r += (4.0 / 420.0) * w[1];
+template <typename T>
+__host__ __device__ inline T upwind7_right(const T w[8]) {
+  T r = T(0.0);
+  r += T(-3.0 / 420.0) * w[7];
+  r += T(25.0 / 420.0) * w[6];
+  r += T(-101.0 / 420.0) * w[5];
+  r += T(319.0 / 420.0) * w[4];
+  r += T(214.0 / 420.0) * w[3];
+  r += T(-38.0 / 420.0) * w[2];
+  r += T(4.0 / 420.0) * w[1];
   return r;
 }
 
 // nonorthogonal_reconstruction.c:36-51 (Fortran SIGN(1,x) == copysign)
-__host__ __device__ inline double pdm_left(double q0, double q1, double q2,
-                                           double interpolated, double pdmb) {
-  const double bounded = fmax(fmin(q1, q2), fmin(interpolated, fmax(q1, q2)));
-  const double delta0 = pdmb * (q1 - q0);
-  const double delta1 = pdmb * (q2 - q1);
-  const double sign0 = copysign(1.0, delta0);
-  const double sign1 = copysign(1.0, delta1);
-  const double same = fabs(sign0 + sign1);
-  const double slope = bounded - q1;
-  return bounded - sign1 * fmax(0.0, fabs(slope) - same * fabs(delta0));
+template <typename T>
+__host__ __device__ inline T pdm_left(T q0, T q1, T q2, T interpolated, T pdmb) {
+  const T bounded = fmax(fmin(q1, q2), fmin(interpolated, fmax(q1, q2)));
+  const T delta0 = pdmb * (q1 - q0);
+  const T delta1 = pdmb * (q2 - q1);
+  const T sign0 = copysign(T(1.0), delta0);
+  const T sign1 = copysign(T(1.0), delta1);
+  const T same = fabs(sign0 + sign1);
+  const T slope = bounded - q1;
+  return bounded - sign1 * fmax(T(0.0), fabs(slope) - same * fabs(delta0));
 }
 
 // nonorthogonal_reconstruction.c:61-93 with the interface volume
@@ -110,15 +134,14 @@ __host__ __device__ inline void up7_pdm(const double vol[8], const double q[8],
 // up7_pdm with the division by the interface volume replaced by a multiply
 // with its reciprocal (computed once per face for all eight variables):
 // the high-order value may differ from the reference's by one rounding.
-__host__ __device__ inline void up7_pdm_rcp(const double vol[8],
-                                            const double q[8], double riv,
-                                            double pdmb, double *left,
-                                            double *right) {
-  double w[8];
+template <typename T>
+__host__ __device__ inline void up7_pdm_rcp(const T vol[8], const T q[8], T riv,
+                                            T pdmb, T *left, T *right) {
+  T w[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) w[n] = vol[n] * q[n];
-  const double hl = upwind7_left(w) * riv;
-  const double hr = upwind7_right(w) * riv;
+  const T hl = upwind7_left(w) * riv;
+  const T hr = upwind7_right(w) * riv;
   *left = pdm_left(q[2], q[3], q[4], hl, pdmb);
   *right = pdm_left(q[5], q[4], q[3], hr, pdmb);
 }
@@ -184,58 +207,62 @@ __host__ __device__ inline int predict_cell(const double uold[5],
 }
 
 // nonorthogonal_flux.c:25-36
-__host__ __device__ inline bool valid_prim(const Prim &s) {
-  if (!isfinite(s.rho) || !isfinite(s.p) || s.rho <= DBL_MIN ||
-      s.p <= DBL_MIN)
+template <typename T>
+__host__ __device__ inline bool valid_prim(const PrimT<T> &s) {
+  if (!isfinite(s.rho) || !isfinite(s.p) || s.rho <= Num<T>::tiny ||
+      s.p <= Num<T>::tiny)
     return false;
   return isfinite(s.vx) && isfinite(s.vy) && isfinite(s.vz);
 }
 
+template <typename T>
 struct FaceFrame {
-  double nx, ny, nz, t1x, t1y, t1z, t2x, t2y, t2z;
+  T nx, ny, nz, t1x, t1y, t1z, t2x, t2y, t2z;
 };
 
+template <typename T>
 struct FluidFlux {
-  double f[5];
-  double jump[5];
-  double vjump[3];
-  double vn[2];
+  T f[5];
+  T jump[5];
+  T vjump[3];
+  T vn[2];
 };
 
 // nonorthogonal_flux.c:38-105
-__device__ inline int kinetic_fluid_flux(const Prim st[2], double gamma,
-                                         const FaceFrame &fr, FluidFlux *fl) {
-  if (!isfinite(gamma) || gamma <= 1.0 || !valid_prim(st[0]) ||
+template <typename T>
+__device__ inline int kinetic_fluid_flux(const PrimT<T> st[2], T gamma,
+                                         const FaceFrame<T> &fr, FluidFlux<T> *fl) {
+  if (!isfinite(gamma) || gamma <= T(1.0) || !valid_prim(st[0]) ||
       !valid_prim(st[1]))
     return 1;
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
-    fl->f[m] = 0.0;
-    fl->jump[m] = 0.0;
+    fl->f[m] = T(0.0);
+    fl->jump[m] = T(0.0);
   }
-  fl->vjump[0] = fl->vjump[1] = fl->vjump[2] = 0.0;
-  const double pi = 3.14159265358979323846264338327950288;
+  fl->vjump[0] = fl->vjump[1] = fl->vjump[2] = T(0.0);
+  const T pi = T(3.14159265358979323846264338327950288);
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
-    const double sign = side == 0 ? -1.0 : 1.0;
-    const double rho = st[side].rho;
-    const double p = st[side].p;
-    const double vx = st[side].vx, vy = st[side].vy, vz = st[side].vz;
-    const double v2 = dot3(vx, vy, vz, vx, vy, vz);
-    const double energy = 0.5 * rho * v2 + p / (gamma - 1.0);
-    const double lambda = rho / (2.0 * p);
-    const double vn = dot3(fr.nx, fr.ny, fr.nz, vx, vy, vz);
-    const double vt1 = dot3(fr.t1x, fr.t1y, fr.t1z, vx, vy, vz);
-    const double vt2 = dot3(fr.t2x, fr.t2y, fr.t2z, vx, vy, vz);
-    const double zeroth = 0.5 * erfc(sign * sqrt(lambda) * vn);
-    const double first =
-        vn * zeroth - 0.5 * sign * exp(-lambda * vn * vn) / sqrt(pi * lambda);
+    const T sign = side == 0 ? T(-1.0) : T(1.0);
+    const T rho = st[side].rho;
+    const T p = st[side].p;
+    const T vx = st[side].vx, vy = st[side].vy, vz = st[side].vz;
+    const T v2 = dot3(vx, vy, vz, vx, vy, vz);
+    const T energy = T(0.5) * rho * v2 + p / (gamma - T(1.0));
+    const T lambda = rho / (T(2.0) * p);
+    const T vn = dot3(fr.nx, fr.ny, fr.nz, vx, vy, vz);
+    const T vt1 = dot3(fr.t1x, fr.t1y, fr.t1z, vx, vy, vz);
+    const T vt2 = dot3(fr.t2x, fr.t2y, fr.t2z, vx, vy, vz);
+    const T zeroth = T(0.5) * Num<T>::erfc_(sign * Num<T>::sqrt_(lambda) * vn);
+    const T first = vn * zeroth - T(0.5) * sign * Num<T>::exp_(-lambda * vn * vn) /
+                                      Num<T>::sqrt_(pi * lambda);
     fl->vn[side] = vn;
     fl->f[0] += rho * first;
-    fl->f[4] += (energy + 0.5 * p) * first + 0.5 * p * zeroth * vn;
-    const double mn = rho * vn * first + p * zeroth;
-    const double mt1 = rho * vt1 * first;
-    const double mt2 = rho * vt2 * first;
+    fl->f[4] += (energy + T(0.5) * p) * first + T(0.5) * p * zeroth * vn;
+    const T mn = rho * vn * first + p * zeroth;
+    const T mt1 = rho * vt1 * first;
+    const T mt2 = rho * vt2 * first;
     fl->f[1] += fr.nx * mn + fr.t1x * mt1 + fr.t2x * mt2;
     fl->vjump[0] += sign * vx;
     fl->f[2] += fr.ny * mn + fr.t1y * mt1 + fr.t2y * mt2;
@@ -251,18 +278,20 @@ __device__ inline int kinetic_fluid_flux(const Prim st[2], double gamma,
   return 0;
 }
 
+template <typename T>
 struct MaxwellFlux {
-  double m[3];
-  double alfven;
-  double pmag;
+  T m[3];
+  T alfven;
+  T pmag;
 };
 
 // nonorthogonal_flux.c:107-173
-__device__ inline int kinetic_maxwell_flux(
-    const Prim st[2], const double b[2][3], double bn, const FaceFrame &fr,
-    bool use_bg, const double b0[3], double b0n, bool use_boris, double c,
-    const double vn[2], MaxwellFlux *mx) {
-  if (!isfinite(bn) || (use_boris && (!isfinite(c) || c <= DBL_MIN))) return 1;
+template <typename T>
+__device__ inline int kinetic_maxwell_flux(const PrimT<T> st[2], const T b[2][3], T bn,
+                                           const FaceFrame<T> &fr, bool use_bg,
+                                           const T b0[3], T b0n, bool use_boris, T c,
+                                           const T vn[2], MaxwellFlux<T> *mx) {
+  if (!isfinite(bn) || (use_boris && (!isfinite(c) || c <= Num<T>::tiny))) return 1;
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
     if (!valid_prim(st[side])) return 1;
@@ -270,37 +299,35 @@ __device__ inline int kinetic_maxwell_flux(
     for (int d = 0; d < 3; ++d)
       if (!isfinite(b[side][d]) || (use_bg && !isfinite(b0[d]))) return 1;
   }
-  mx->m[0] = mx->m[1] = mx->m[2] = 0.0;
-  mx->alfven = 0.0;
-  mx->pmag = 0.0;
-  const double nrm[3] = {fr.nx, fr.ny, fr.nz};
+  mx->m[0] = mx->m[1] = mx->m[2] = T(0.0);
+  mx->alfven = T(0.0);
+  mx->pmag = T(0.0);
+  const T nrm[3] = {fr.nx, fr.ny, fr.nz};
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
-    const double sign = side == 0 ? -1.0 : 1.0;
-    const double r2 = dot3(b[side][0], b[side][1], b[side][2], b[side][0],
-                           b[side][1], b[side][2]);
-    const double rp = 0.5 * r2;
-    double tx = b[side][0], ty = b[side][1], tz = b[side][2];
+    const T sign = side == 0 ? T(-1.0) : T(1.0);
+    const T r2 = dot3(b[side][0], b[side][1], b[side][2], b[side][0], b[side][1],
+                      b[side][2]);
+    const T rp = T(0.5) * r2;
+    T tx = b[side][0], ty = b[side][1], tz = b[side][2];
     if (use_bg) {
       tx = b[side][0] + b0[0];
       ty = b[side][1] + b0[1];
       tz = b[side][2] + b0[2];
     }
-    const double t2 = dot3(tx, ty, tz, tx, ty, tz);
-    const double va2 = t2 / st[side].rho;
-    const double cva2 = use_boris ? va2 / (1.0 + va2 / (c * c)) : va2;
-    const double lambda = 1.0 / (2.0 * st[side].p / st[side].rho + cva2);
-    const double zeroth = 0.5 * erfc(sign * sqrt(lambda) * vn[side]);
-    mx->alfven += 0.5 * sqrt(cva2);
-    mx->pmag += 0.5 * t2;
-    const double bdr =
-        use_bg ? dot3(b0[0], b0[1], b0[2], b[side][0], b[side][1], b[side][2])
-               : 0.0;
+    const T t2 = dot3(tx, ty, tz, tx, ty, tz);
+    const T va2 = t2 / st[side].rho;
+    const T cva2 = use_boris ? va2 / (T(1.0) + va2 / (c * c)) : va2;
+    const T lambda = T(1.0) / (T(2.0) * st[side].p / st[side].rho + cva2);
+    const T zeroth = T(0.5) * Num<T>::erfc_(sign * Num<T>::sqrt_(lambda) * vn[side]);
+    mx->alfven += T(0.5) * Num<T>::sqrt_(cva2);
+    mx->pmag += T(0.5) * t2;
+    const T bdr =
+        use_bg ? dot3(b0[0], b0[1], b0[2], b[side][0], b[side][1], b[side][2]) : T(0.0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      double stress = rp * nrm[d] - b[side][d] * bn;
-      if (use_bg)
-        stress += -b0[d] * bn - b[side][d] * b0n + bdr * nrm[d];
+      T stress = rp * nrm[d] - b[side][d] * bn;
+      if (use_bg) stress += -b0[d] * bn - b[side][d] * b0n + bdr * nrm[d];
       mx->m[d] += zeroth * stress;
     }
   }
@@ -308,36 +335,37 @@ __device__ inline int kinetic_maxwell_flux(
 }
 
 // nonorthogonal_flux.c:175-204 (options were validated at entry)
-__device__ inline void apply_hogs(FluidFlux *fl, MaxwellFlux *mx, double ch,
-                                  double cm, bool use_boris, double c) {
+template <typename T>
+__device__ inline void apply_hogs(FluidFlux<T> *fl, MaxwellFlux<T> *mx, T ch, T cm,
+                                  bool use_boris, T c) {
 #pragma unroll
   for (int m = 0; m < 5; ++m) fl->f[m] -= ch * mx->alfven * fl->jump[m];
   if (use_boris) {
-    const double ic2 = 1.0 / (c * c);
+    const T ic2 = T(1.0) / (c * c);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double j = mx->pmag * fl->vjump[d] * ic2;
+      const T j = mx->pmag * fl->vjump[d] * ic2;
       mx->m[d] -= cm * mx->alfven * j;
     }
   }
 }
 
 // nonorthogonal_flux.c:206-241 (use_boris is true at every call site)
-__device__ inline int emergency_diffusion(FluidFlux *fl, const Prim st[2],
-                                          const double lo[5],
-                                          const double hi[5], double c,
-                                          bool *applied, double *speed) {
+template <typename T>
+__device__ inline int emergency_diffusion(FluidFlux<T> *fl, const PrimT<T> st[2],
+                                          const T lo[5], const T hi[5], T c,
+                                          bool *applied, T *speed) {
   *applied = false;
-  double s2 = 0.0;
+  T s2 = T(0.0);
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
     if (!valid_prim(st[side])) return 1;
-    s2 += dot3(st[side].vx, st[side].vy, st[side].vz, st[side].vx,
-               st[side].vy, st[side].vz);
+    s2 += dot3(st[side].vx, st[side].vy, st[side].vz, st[side].vx, st[side].vy,
+               st[side].vz);
   }
-  const double is = sqrt(0.5 * s2);
+  const T is = Num<T>::sqrt_(T(0.5) * s2);
   *speed = is;
-  if (is < 1.5 * c) return 0;
+  if (is < T(1.5) * c) return 0;
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
     if (!isfinite(lo[m]) || !isfinite(hi[m])) return 1;
@@ -348,19 +376,18 @@ __device__ inline int emergency_diffusion(FluidFlux *fl, const Prim st[2],
 }
 
 // nonorthogonal_operators.c:144-182 (length > DBL_MIN checked at set-up)
-__device__ inline int edge_emf(double vt1, double vt2, double bt1, double bt2,
-                               double jump, double rho, double length,
-                               double diffusion, bool use_boris, double c,
-                               double cfl, double dt, double *emf) {
+template <typename T>
+__device__ inline int edge_emf(T vt1, T vt2, T bt1, T bt2, T jump, T rho, T length,
+                               T diffusion, bool use_boris, T c, T cfl, T dt, T *emf) {
   if (!isfinite(vt1) || !isfinite(vt2) || !isfinite(bt1) || !isfinite(bt2) ||
-      !isfinite(jump) || !isfinite(rho) || rho <= DBL_MIN)
+      !isfinite(jump) || !isfinite(rho) || rho <= Num<T>::tiny)
     return 1;
-  const double flow = hypot(vt1, vt2);
-  double va = hypot(bt1, bt2) / sqrt(rho);
-  if (use_boris) va = c * va / hypot(c, va);
-  double speed = flow + va;
+  const T flow = Num<T>::hypot_(vt1, vt2);
+  T va = Num<T>::hypot_(bt1, bt2) / Num<T>::sqrt_(rho);
+  if (use_boris) va = c * va / Num<T>::hypot_(c, va);
+  T speed = flow + va;
   speed = fmin(speed, cfl * length / dt);
-  const double ideal = -(vt1 * bt2 - vt2 * bt1);
+  const T ideal = -(vt1 * bt2 - vt2 * bt1);
   *emf = (ideal + diffusion * speed * jump) * length;
   return 0;
 }

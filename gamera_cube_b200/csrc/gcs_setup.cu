@@ -325,6 +325,8 @@ void Context::release() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   graph_exec = nullptr;
   if (pool) cudaFree(pool);
+  if (bulk_pool) cudaFree(bulk_pool);
+  bulk_pool = nullptr;
   if (bg_pool) cudaFree(bg_pool);
   bg_pool = nullptr;
   if (plans) cudaFree(plans);
@@ -798,6 +800,168 @@ int Context::read_status(DevStatus *out) {
   GCS_TRY(cudaMemcpyAsync(out, X.status, sizeof(DevStatus),
                           cudaMemcpyDeviceToHost, stream));
   GCS_TRY(cudaStreamSynchronize(stream));
+  return 0;
+}
+
+}  // namespace gcs
+
+namespace gcs {
+
+namespace {
+
+__global__ void k_to_f32(const double *src, float *dst, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = (float)src[t];
+}
+
+__global__ void k_layer_b0(Dims D, DevBg BG, unsigned long long *layer_max) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long cells = (long long)D.E0 * D.E1 * D.E2;
+  if (t >= kFaces * cells) return;
+  const int f = (int)(t / cells);
+  const long long r = t - f * cells;
+  const int i = (int)(r / ((long long)D.E1 * D.E2));
+  const int j = (int)((r / D.E2) % D.E1), k = (int)(r % D.E2);
+  const long long c = f * D.Nn + D.node(i, j, k);
+  const double b = sqrt(BG.b0[0][c] * BG.b0[0][c] + BG.b0[1][c] * BG.b0[1][c] +
+                        BG.b0[2][c] * BG.b0[2][c]);
+  if (isfinite(b)) atomicMax(&layer_max[i], (unsigned long long)__double_as_longlong(b));
+}
+
+}  // namespace
+
+// FP32 arrays of the bulk path, one per node per component: 14 sweep
+// inputs (Pr 5, Bp 3, BN 3, W 3), 76 metric (vol, iv 3, area 3, face
+// frames 27, edge length 3, edge tangents 18, transverse normals 12,
+// 1/det 3, central face areas 6) and 18 background (face B0 9, face B0
+// normal 3, edge B0 projections 6).  The sweep outputs stay the FP64
+// arrays of the state.
+int Context::enable_bulk(int on) {
+  if (!on) {
+    X.bulk = 0;
+    return 0;
+  }
+  const long long n = (long long)kFaces * X.D.Nn;
+  const int arrays = 14 + 76 + 18;
+  if (!bulk_pool) {
+    bulk_bytes = (size_t)arrays * n * sizeof(float);
+    if (cudaMalloc(&bulk_pool, bulk_bytes) != cudaSuccess) {
+      bulk_pool = nullptr;
+      set_error("cannot allocate the FP32 arrays", "enable_bulk");
+      return -1;
+    }
+    cudaMemsetAsync(bulk_pool, 0, bulk_bytes, stream);
+    float *q = (float *)bulk_pool;
+    auto take = [&]() {
+      float *r = q;
+      q += n;
+      return r;
+    };
+    Bulk<float> &B = X.B32;
+    for (int m = 0; m < 5; ++m) B.Pr[m] = take();
+    for (int d = 0; d < 3; ++d) {
+      B.Bp[d] = take();
+      B.BN[d] = take();
+      B.W[d] = take();
+      B.E[d] = X.S.E[d];
+      for (int m = 0; m < 3; ++m) B.FV[d][m] = X.S.FV[d][m];
+      for (int m = 0; m < 5; ++m) B.F[d][m] = X.S.F[d][m];
+      for (int m = 0; m < 3; ++m) B.M[d][m] = X.S.M[d][m];
+    }
+    const DevGeom &G = X.G;
+    const int bs = 256;
+    const unsigned nb = (unsigned)((n + bs - 1) / bs);
+    auto conv = [&](const double *src) -> const float * {
+      float *dst = take();
+      if (src) k_to_f32<<<nb, bs, 0, stream>>>(src, dst, n);
+      return dst;
+    };
+    B.vol = conv(G.vol);
+    for (int d = 0; d < 3; ++d) {
+      B.iv[d] = conv(G.iv[d]);
+      B.area[d] = conv(G.area[d]);
+      B.elen[d] = conv(G.elen[d]);
+      B.einv[d] = conv(G.einv[d]);
+      B.ca[d] = conv(G.ca[d]);
+      B.cb[d] = conv(G.cb[d]);
+      for (int m = 0; m < 3; ++m) {
+        B.fn[d][m] = conv(G.fn[d][m]);
+        B.ft1[d][m] = conv(G.ft1[d][m]);
+        B.ft2[d][m] = conv(G.ft2[d][m]);
+        B.et1[d][m] = conv(G.et1[d][m]);
+        B.et2[d][m] = conv(G.et2[d][m]);
+      }
+      for (int m = 0; m < 2; ++m) {
+        B.en1[d][m] = conv(G.en1[d][m]);
+        B.en2[d][m] = conv(G.en2[d][m]);
+      }
+    }
+    for (int d = 0; d < 3; ++d) {
+      B.fb0n[d] = take();
+      B.eb0t1[d] = take();
+      B.eb0t2[d] = take();
+      for (int m = 0; m < 3; ++m) B.fb0[d][m] = take();
+    }
+    bulk_bg_dirty = 1;
+  }
+  if (bulk_bg_dirty) {
+    // the background's FP32 copies follow every background upload
+    const DevBg &BG = X.BG;
+    Bulk<float> &B = X.B32;
+    const int bs = 256;
+    const unsigned nb = (unsigned)((n + bs - 1) / bs);
+    auto conv = [&](const double *src, const float *dst) {
+      if (src) k_to_f32<<<nb, bs, 0, stream>>>(src, (float *)dst, n);
+    };
+    for (int d = 0; d < 3; ++d) {
+      conv(BG.fb0n[d], B.fb0n[d]);
+      conv(BG.eb0t1[d], B.eb0t1[d]);
+      conv(BG.eb0t2[d], B.eb0t2[d]);
+      for (int m = 0; m < 3; ++m) conv(BG.fb0[d][m], B.fb0[d][m]);
+    }
+    bulk_bg_dirty = 0;
+  }
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
+    set_error("FP32 conversion failed", "enable_bulk");
+    return -1;
+  }
+  if (set_bulk_split(bulk_b0_threshold) != 0) return -1;
+  X.bulk = 1;
+  return 0;
+}
+
+// Radial layers whose largest cell |B0| exceeds the threshold, and all
+// layers inside them, keep the FP64 sweeps.
+int Context::set_bulk_split(double b0_threshold) {
+  bulk_b0_threshold = b0_threshold;
+  const Dims &D = X.D;
+  X.bulk_split = 0;
+  if (X.BG.b0[0] == nullptr) return 0;
+  unsigned long long *dmax = nullptr;
+  std::vector<unsigned long long> hmax(D.E0, 0ULL);
+  const long long cells = (long long)kFaces * D.E0 * D.E1 * D.E2;
+  if (cudaMalloc(&dmax, D.E0 * sizeof(unsigned long long)) != cudaSuccess) {
+    set_error("cannot allocate", "set_bulk_split");
+    return -1;
+  }
+  cudaMemsetAsync(dmax, 0, D.E0 * sizeof(unsigned long long), stream);
+  k_layer_b0<<<(unsigned)((cells + 255) / 256), 256, 0, stream>>>(D, X.BG, dmax);
+  const bool ok = cudaMemcpyAsync(hmax.data(), dmax, D.E0 * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, stream) == cudaSuccess &&
+                  cudaStreamSynchronize(stream) == cudaSuccess;
+  cudaFree(dmax);
+  if (!ok) {
+    set_error("layer B0 reduction failed", "set_bulk_split");
+    return -1;
+  }
+  for (int i = D.E0 - 1; i >= 0; --i) {
+    double b;
+    memcpy(&b, &hmax[i], sizeof(b));
+    if (b > b0_threshold) {
+      X.bulk_split = i + 1;
+      break;
+    }
+  }
   return 0;
 }
 

@@ -310,6 +310,25 @@ size_t gcs_noalloc_scratch_bytes(void);
 gcs_context *gcs_halo_plan_context(gamera_cs_halo_plan *plan);
 int gcs_context_set_resident(gcs_context *ctx, int on);
 
+/* FP32-bulk precision variant (no reference counterpart).  With fp32_bulk
+ * set, the flux, face-velocity and edge-EMF sweeps compute in FP32 from
+ * FP32 copies of the metric, background, cell primitives and face fields
+ * (outside the strong-dipole layers, below) and store FP64 results; the
+ * conserved state, face B flux, predictor, B recovery, CT and cell update
+ * stay FP64, so div B stays at FP64 round-off.  The FP32 copies (108
+ * floats per node) are allocated and converted on first use and follow
+ * later background uploads.  Host callbacks need the FP64 path. */
+int gcs_context_set_precision(gcs_context *ctx, int fp32_bulk);
+int gcs_context_precision(const gcs_context *ctx);
+/* Radial layers whose largest cell |B0| exceeds b0_threshold (code units,
+ * default 8), and every layer inside them, keep the FP64 sweeps in the
+ * FP32-bulk path: there the residual field is small against the dipole and
+ * FP32 rounding of the B0 cross terms of the Maxwell stress and EMF would
+ * dominate their differences.  gcs_context_bulk_split returns the first
+ * FP32 radial layer (cell index, ghosts included). */
+int gcs_context_set_bulk_threshold(gcs_context *ctx, double b0_threshold);
+int gcs_context_bulk_split(const gcs_context *ctx);
+
 /* Device-resident ionosphere solves (no reference counterpart).  A plan
  * holds `count` independent systems on one polar grid (for example the two
  * hemispheres, configs differing in `hemisphere`); one solve launch runs

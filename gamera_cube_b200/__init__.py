@@ -106,6 +106,22 @@ def _load(path=None):
     sig["gcs_context_precision"] = (C.c_int, [C.c_void_p])
     sig["gcs_context_set_bulk_threshold"] = (C.c_int, [C.c_void_p, C.c_double])
     sig["gcs_context_bulk_split"] = (C.c_int, [C.c_void_p])
+    c_sz3p = P(C.c_size_t)
+    for name in ("gamera_cs_fill_tangential_cell_halos", "gamera_cs_fill_magnetic_face_halos",
+                 "gamera_cs_sync_edge_emf"):
+        sig[name] = (C.c_int, [P(abi.Grid), P(abi.Storage), c_sz3p, C.c_size_t])
+    for name in ("gamera_cs_fill_radial_outflow_cells", "gamera_cs_sync_magnetic_face_flux",
+                 "gamera_cs_sync_mhd_face_fluxes"):
+        sig[name] = (C.c_int, [P(abi.Storage), c_sz3p, C.c_size_t])
+    sig["gamera_cs_fill_radial_outflow_cells_face"] = (
+        C.c_int, [P(abi.Storage), c_sz3p, C.c_size_t, C.c_int])
+    for name in ("gamera_cs_fill_tangential_cell_halos_planned_face",
+                 "gamera_cs_fill_magnetic_face_halos_planned_face"):
+        sig[name] = (C.c_int, [C.c_void_p, P(abi.Grid), P(abi.Storage), C.c_int])
+    sig["gamera_cs_edge_sync_plan_create"] = (C.c_int, [P(abi.Grid), c_sz3p, C.c_size_t,
+                                                        P(C.c_void_p)])
+    sig["gamera_cs_edge_sync_plan_destroy"] = (None, [C.c_void_p])
+    sig["gamera_cs_sync_edge_emf_planned"] = (C.c_int, [C.c_void_p, P(abi.Storage)])
     sig.update(abi.mi_dipole_signatures())
     sig["gcs_context_mi_dipole_create"] = (
         C.c_int, [C.c_void_p, P(abi.EarthStartup), P(abi.MiDipoleConfig),

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
 #include <mutex>
 #include <new>
@@ -20,6 +21,10 @@ struct gcs_context {
 };
 
 struct gamera_cs_halo_plan {
+  gcs_context *ctx;
+};
+
+struct gamera_cs_edge_sync_plan {
   gcs_context *ctx;
 };
 
@@ -405,6 +410,132 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
   return (rc != 0 || fail) ? -1 : 0;
 }
 
+// ---- stand-alone halo and seam entry points -------------------------------
+
+// Downloads of one face (receiver >= 0) or all faces.
+int download_arrays(gcs::Context &C, gamera_no_storage *st, const int *kinds, int nk,
+                    int receiver) {
+  for (int f = 0; f < gcs::kFaces; ++f) {
+    if (receiver >= 0 && f != receiver) continue;
+    for (int q = 0; q < nk; ++q) {
+      const int kind = kinds[q];
+      int dirs = (kind == gcs::kArrP || kind == gcs::kArrPo || kind == gcs::kArrF ||
+                  kind == gcs::kArrM || kind == gcs::kArrE) ? 3 : 1;
+      for (int d = 0; d < dirs; ++d) {
+        double *host = nullptr;
+        switch (kind) {
+          case gcs::kArrU: host = st[f].conserved; break;
+          case gcs::kArrUo: host = st[f].old_conserved; break;
+          case gcs::kArrB: host = (double *)st[f].cell_magnetic; break;
+          case gcs::kArrBo: host = (double *)st[f].old_cell_magnetic; break;
+          case gcs::kArrP: host = st[f].face_flux[d]; break;
+          case gcs::kArrPo: host = st[f].old_face_flux[d]; break;
+          case gcs::kArrF: host = st[f].fluid_face_flux[d]; break;
+          case gcs::kArrM: host = (double *)st[f].maxwell_face_flux[d]; break;
+          case gcs::kArrE: host = st[f].edge_emf[d]; break;
+          default: return -1;
+        }
+        if (C.transfer_array(f, kind, d, false, host) != 0) return -1;
+      }
+    }
+  }
+  return 0;
+}
+
+int upload_arrays(gcs::Context &C, gamera_no_storage *st, const int *kinds, int nk) {
+  for (int f = 0; f < gcs::kFaces; ++f)
+    for (int q = 0; q < nk; ++q) {
+      const int kind = kinds[q];
+      int dirs = (kind == gcs::kArrP || kind == gcs::kArrPo || kind == gcs::kArrF ||
+                  kind == gcs::kArrM || kind == gcs::kArrE) ? 3 : 1;
+      for (int d = 0; d < dirs; ++d) {
+        double *host = nullptr;
+        switch (kind) {
+          case gcs::kArrU: host = st[f].conserved; break;
+          case gcs::kArrUo: host = st[f].old_conserved; break;
+          case gcs::kArrB: host = (double *)st[f].cell_magnetic; break;
+          case gcs::kArrBo: host = (double *)st[f].old_cell_magnetic; break;
+          case gcs::kArrP: host = st[f].face_flux[d]; break;
+          case gcs::kArrPo: host = st[f].old_face_flux[d]; break;
+          case gcs::kArrF: host = st[f].fluid_face_flux[d]; break;
+          case gcs::kArrM: host = (double *)st[f].maxwell_face_flux[d]; break;
+          case gcs::kArrE: host = st[f].edge_emf[d]; break;
+          default: return -1;
+        }
+        if (C.transfer_array(f, kind, d, true, host) != 0) return -1;
+      }
+    }
+  return 0;
+}
+
+const int kCellArrays[4] = {gcs::kArrU, gcs::kArrUo, gcs::kArrB, gcs::kArrBo};
+const int kFaceArrays[2] = {gcs::kArrP, gcs::kArrPo};
+
+bool dims_match(const gcs::Context &C, const size_t active[3], size_t ghost) {
+  return active && (size_t)C.X.D.nr == active[0] && (size_t)C.X.D.n == active[1] &&
+         (size_t)C.X.D.n == active[2] && (size_t)C.X.D.g == ghost;
+}
+
+bool storage_matches(const gcs::Context &C, const gamera_no_storage *st) {
+  for (int f = 0; f < gcs::kFaces; ++f)
+    if (st[f].cell_extent[0] != (size_t)C.X.D.E0 ||
+        st[f].cell_extent[1] != (size_t)C.X.D.E1 ||
+        st[f].cell_extent[2] != (size_t)C.X.D.E2)
+      return false;
+  return true;
+}
+
+int cell_halos(gcs::Context &C, gamera_no_storage *st, int receiver) {
+  if (upload_arrays(C, st, kCellArrays, 4) != 0) return -1;
+  C.reset_status_async();
+  gcs::launch_halo_cells_only(C.X, C.stream);
+  if (cudaStreamSynchronize(C.stream) != cudaSuccess) return -1;
+  return download_arrays(C, st, kCellArrays, 4, receiver);
+}
+
+int face_halos(gcs::Context &C, gamera_no_storage *st, int receiver) {
+  const int kinds[6] = {gcs::kArrB, gcs::kArrBo, gcs::kArrP, gcs::kArrPo};
+  if (upload_arrays(C, st, kinds, 4) != 0) return -1;
+  C.reset_status_async();
+  gcs::launch_halo_faces_only(C.X, C.stream);
+  if (cudaStreamSynchronize(C.stream) != cudaSuccess) return -1;
+  return download_arrays(C, st, kFaceArrays, 2, receiver);
+}
+
+// Contexts without a grid (state arrays, seams and edge groups only) for
+// the entry points that take storage alone, one per active extent.
+std::mutex g_topo_mutex;
+std::map<std::array<size_t, 4>, gcs_context *> g_topo;
+
+gcs_context *topology_context(const size_t active[3], size_t ghost) {
+  if (!active) return nullptr;
+  std::lock_guard<std::mutex> lock(g_topo_mutex);
+  const std::array<size_t, 4> key{active[0], active[1], active[2], ghost};
+  auto it = g_topo.find(key);
+  if (it != g_topo.end()) return it->second;
+  gcs_context *ctx = new (std::nothrow) gcs_context;
+  if (!ctx) return nullptr;
+  if (ctx->c.init_topology(active, ghost) != 0) {
+    set_last(ctx->c.error);
+    delete ctx;
+    return nullptr;
+  }
+  g_topo[key] = ctx;
+  return ctx;
+}
+
+int radial_outflow(gamera_no_storage storage[6], const size_t active[3], size_t ghost,
+                   int receiver) {
+  if (!storage || !active || ghost < 4 || active[0] == 0) return -1;
+  gcs_context *ctx = topology_context(active, ghost);
+  if (!ctx || !storage_matches(ctx->c, storage)) return -1;
+  gcs::Context &C = ctx->c;
+  if (upload_arrays(C, storage, kCellArrays, 4) != 0) return -1;
+  gcs::launch_radial_outflow_all(C.X, C.stream);
+  if (cudaStreamSynchronize(C.stream) != cudaSuccess) return -1;
+  return download_arrays(C, storage, kCellArrays, 4, receiver);
+}
+
 }  // namespace
 
 namespace gcs {
@@ -526,6 +657,132 @@ int gamera_cs_halo_valid_state(const double state[5]) {
     m2 += m * m;
   }
   return std::isfinite(state[4]) && state[4] > 0.5 * m2 / rho;
+}
+
+// cubedsphere_halo.h:52-59
+int gamera_cs_fill_tangential_cell_halos_planned_face(const gamera_cs_halo_plan *plan,
+                                                      const gamera_no_grid grid[6],
+                                                      gamera_no_storage storage[6],
+                                                      int receiver) {
+  if (!plan || !grid || !storage || receiver < 0 || receiver >= 6 ||
+      !plan->ctx->c.grid_matches(grid))
+    return -1;
+  return cell_halos(plan->ctx->c, storage, receiver);
+}
+
+int gamera_cs_fill_magnetic_face_halos_planned_face(const gamera_cs_halo_plan *plan,
+                                                    const gamera_no_grid grid[6],
+                                                    gamera_no_storage storage[6],
+                                                    int receiver) {
+  if (!plan || !grid || !storage || receiver < 0 || receiver >= 6 ||
+      !plan->ctx->c.grid_matches(grid))
+    return -1;
+  return face_halos(plan->ctx->c, storage, receiver);
+}
+
+// cubedsphere_halo.h:68-71 (the device plan of the grid is built on first use)
+int gamera_cs_fill_tangential_cell_halos(const gamera_no_grid grid[6],
+                                         gamera_no_storage storage[6],
+                                         const size_t active[3], size_t ghost) {
+  if (!grid || !storage || !active) return -1;
+  gcs_context *ctx = context_for(grid, active, ghost);
+  if (!ctx || !dims_match(ctx->c, active, ghost) || !storage_matches(ctx->c, storage))
+    return -1;
+  return cell_halos(ctx->c, storage, -1);
+}
+
+// cubedsphere_halo.h:84-87
+int gamera_cs_fill_magnetic_face_halos(const gamera_no_grid grid[6],
+                                       gamera_no_storage storage[6],
+                                       const size_t active[3], size_t ghost) {
+  if (!grid || !storage || !active) return -1;
+  gcs_context *ctx = context_for(grid, active, ghost);
+  if (!ctx || !dims_match(ctx->c, active, ghost) || !storage_matches(ctx->c, storage))
+    return -1;
+  return face_halos(ctx->c, storage, -1);
+}
+
+// cubedsphere_halo.h:74-79
+int gamera_cs_fill_radial_outflow_cells(gamera_no_storage storage[6],
+                                        const size_t active[3], size_t ghost) {
+  return radial_outflow(storage, active, ghost, -1);
+}
+
+int gamera_cs_fill_radial_outflow_cells_face(gamera_no_storage storage[6],
+                                             const size_t active[3], size_t ghost,
+                                             int receiver) {
+  if (receiver < 0 || receiver >= 6) return -1;
+  return radial_outflow(storage, active, ghost, receiver);
+}
+
+// cubedsphere_interface.h:13-18
+int gamera_cs_sync_magnetic_face_flux(gamera_no_storage storage[6],
+                                      const size_t active[3], size_t ghost) {
+  if (!storage || !active) return -1;
+  gcs_context *ctx = topology_context(active, ghost);
+  if (!ctx || !storage_matches(ctx->c, storage)) return -1;
+  gcs::Context &C = ctx->c;
+  if (upload_arrays(C, storage, kFaceArrays, 2) != 0) return -1;
+  C.reset_status_async();
+  gcs::launch_seam_sync(C.X, 1, C.stream);
+  if (cudaStreamSynchronize(C.stream) != cudaSuccess) return -1;
+  return download_arrays(C, storage, kFaceArrays, 2, -1);
+}
+
+int gamera_cs_sync_mhd_face_fluxes(gamera_no_storage storage[6], const size_t active[3],
+                                   size_t ghost) {
+  if (!storage || !active) return -1;
+  gcs_context *ctx = topology_context(active, ghost);
+  if (!ctx || !storage_matches(ctx->c, storage)) return -1;
+  gcs::Context &C = ctx->c;
+  const int kinds[2] = {gcs::kArrF, gcs::kArrM};
+  if (upload_arrays(C, storage, kinds, 2) != 0) return -1;
+  C.reset_status_async();
+  gcs::launch_seam_sync(C.X, 0, C.stream);
+  if (cudaStreamSynchronize(C.stream) != cudaSuccess) return -1;
+  return download_arrays(C, storage, kinds, 2, -1);
+}
+
+// cubedsphere_interface.h:22-25 and the plan of :29-37 (the plan is the
+// context of the grid; the edge groups are its immutable edge identities)
+int gamera_cs_sync_edge_emf(const gamera_no_grid grid[6], gamera_no_storage storage[6],
+                            const size_t active[3], size_t ghost) {
+  if (!grid || !storage || !active) return -1;
+  gcs_context *ctx = context_for(grid, active, ghost);
+  if (!ctx || !dims_match(ctx->c, active, ghost) || !storage_matches(ctx->c, storage))
+    return -1;
+  gcs::Context &C = ctx->c;
+  const int kinds[1] = {gcs::kArrE};
+  if (upload_arrays(C, storage, kinds, 1) != 0) return -1;
+  C.reset_status_async();
+  gcs::launch_edge_sync(C.X, C.stream);
+  if (cudaStreamSynchronize(C.stream) != cudaSuccess) return -1;
+  return download_arrays(C, storage, kinds, 1, -1);
+}
+
+int gamera_cs_edge_sync_plan_create(const gamera_no_grid grid[6], const size_t active[3],
+                                    size_t ghost, gamera_cs_edge_sync_plan **out) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (!grid || !active) return -1;
+  gcs_context *ctx = context_for(grid, active, ghost);
+  if (!ctx || !dims_match(ctx->c, active, ghost)) return -1;
+  *out = new (std::nothrow) gamera_cs_edge_sync_plan{ctx};
+  return *out ? 0 : -1;
+}
+
+void gamera_cs_edge_sync_plan_destroy(gamera_cs_edge_sync_plan *plan) { delete plan; }
+
+int gamera_cs_sync_edge_emf_planned(const gamera_cs_edge_sync_plan *plan,
+                                    gamera_no_storage storage[6]) {
+  if (!plan || !storage || !storage_matches(plan->ctx->c, storage)) return -1;
+  gcs::Context &C = plan->ctx->c;
+  const int kinds[1] = {gcs::kArrE};
+  if (upload_arrays(C, storage, kinds, 1) != 0) return -1;
+  C.reset_status_async();
+  gcs::launch_edge_sync(C.X, C.stream);
+  if (cudaStreamSynchronize(C.stream) != cudaSuccess) return -1;
+  return download_arrays(C, storage, kinds, 1, -1);
 }
 
 // ------------------------------------------------------------------ Part 2

@@ -59,6 +59,7 @@ struct Context {
   // (gcs_build.cu); no host grid is involved.
   int init_case(int kind, size_t nr, size_t n, unsigned long long seed);
   int allocate(const size_t active[3], size_t ghost);
+  int init_topology(const size_t active[3], size_t ghost);
   int allocate_background();
   // FP32-bulk sweeps on (1) or off (0); the FP32 arrays are allocated and
   // the metric and background converted on first use (gcs_setup.cu).

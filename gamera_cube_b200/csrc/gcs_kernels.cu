@@ -150,6 +150,30 @@ __global__ void k_radial_outflow(Dims D, DevState S, DevStatus *st) {
   }
 }
 
+// Stand-alone radial outflow fill (cubedsphere_halo.c:217-245) over the full
+// tangential extent, ghost columns included.
+__global__ void k_radial_outflow_all(Dims D, DevState S) {
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= D.E1 * D.E2) return;
+  const int f = blockIdx.z;
+  const int gi = blockIdx.y;  // 0 .. 2g-1
+  const int i = gi < D.g ? gi : D.g + D.nr + (gi - D.g);
+  const int j = jk / D.E2, k = jk % D.E2;
+  const int di = gi < D.g ? D.g : D.g + D.nr - 1;
+  const long long x = f * D.Nn + D.node(i, j, k);
+  const long long s = f * D.Nn + D.node(di, j, k);
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    S.U[m][x] = S.U[m][s];
+    S.Uo[m][x] = S.Uo[m][s];
+  }
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    S.B[m][x] = S.B[m][s];
+    S.Bo[m][x] = S.Bo[m][s];
+  }
+}
+
 // Magnetic ghost faces (cubedsphere_halo.c:651-686): interpolated donor B,
 // both time levels, projected on the receiver face's area vector.
 __global__ void k_halo_faces(Dims D, const HaloFace *plan, long long count,
@@ -378,6 +402,11 @@ void launch_halo_faces_only(const Ctx &X, cudaStream_t s) {
   if (X.n_halo_faces)
     k_halo_faces<<<(unsigned)((X.n_halo_faces + 127) / 128), 128, 0, s>>>(
         X.D, X.halo_faces, X.n_halo_faces, X.S, X.status);
+}
+
+void launch_radial_outflow_all(const Ctx &X, cudaStream_t s) {
+  k_radial_outflow_all<<<dim3((X.D.E1 * X.D.E2 + 127) / 128, 2 * X.D.g, kFaces), 128, 0,
+                         s>>>(X.D, X.S);
 }
 
 void launch_halo(const Ctx &X, cudaStream_t s) {

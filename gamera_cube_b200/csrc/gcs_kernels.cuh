@@ -40,6 +40,7 @@ void launch_seam_sync(const Ctx &X, int magnetic, cudaStream_t s);
 void launch_halo(const Ctx &X, cudaStream_t s);
 void launch_halo_cells_only(const Ctx &X, cudaStream_t s);
 void launch_halo_faces_only(const Ctx &X, cudaStream_t s);
+void launch_radial_outflow_all(const Ctx &X, cudaStream_t s);
 void launch_predict(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_flux(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_emf(const Ctx &X, const Opts &O, cudaStream_t s);

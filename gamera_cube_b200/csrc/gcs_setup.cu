@@ -595,6 +595,42 @@ int Context::build_plans(const HaloGeometry &geo) {
   return 0;
 }
 
+// State arrays, seams and edge groups only (no geometry): for the
+// reference entry points that take storage without a grid.
+int Context::init_topology(const size_t active[3], size_t ghost) {
+  if (allocate(active, ghost) != 0) return -1;
+  const Dims &D = X.D;
+  std::vector<Seam> seams;
+  std::vector<int> offsets;
+  std::vector<EdgeMember> members;
+  if (build_seams(D, seams) != 0 || build_edge_groups(D, offsets, members) != 0) {
+    set_error("plan construction failed", "init_topology");
+    return -1;
+  }
+  const size_t b_se = seams.size() * sizeof(Seam);
+  const size_t b_of = offsets.size() * sizeof(int);
+  const size_t b_me = members.size() * sizeof(EdgeMember);
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  plans_bytes = al(b_se) + al(b_of) + al(b_me);
+  GCS_TRY(cudaMalloc(&plans, plans_bytes));
+  char *q = (char *)plans;
+  X.seams = (Seam *)q;
+  q += al(b_se);
+  X.edge_offsets = (int *)q;
+  q += al(b_of);
+  X.edge_members = (EdgeMember *)q;
+  X.n_halo_cells = 0;
+  X.n_halo_faces = 0;
+  X.n_edge_groups = (int)offsets.size() - 1;
+  GCS_TRY(cudaMemcpyAsync(X.seams, seams.data(), b_se, cudaMemcpyHostToDevice, stream));
+  GCS_TRY(cudaMemcpyAsync(X.edge_offsets, offsets.data(), b_of, cudaMemcpyHostToDevice,
+                          stream));
+  GCS_TRY(cudaMemcpyAsync(X.edge_members, members.data(), b_me, cudaMemcpyHostToDevice,
+                          stream));
+  GCS_TRY(cudaStreamSynchronize(stream));
+  return 0;
+}
+
 void convert_cells(const Ctx &X, int f, const gamera_no_cell_geometry *cells,
                    cudaStream_t s) {
   const long long n = (long long)X.D.E0 * X.D.E1 * X.D.E2;

@@ -88,6 +88,49 @@ int gamera_cs_fill_magnetic_face_halos_planned(
 /* cubedsphere/cubedsphere_halo.h:32 */
 int gamera_cs_halo_valid_state(const double state[GAMERA_NO_FLUX_COUNT]);
 
+/* cubedsphere/cubedsphere_halo.h:52-59: as the planned fills, writing only
+ * the receiver face's host arrays. */
+int gamera_cs_fill_tangential_cell_halos_planned_face(
+    const gamera_cs_halo_plan *plan,
+    const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT], int receiver);
+int gamera_cs_fill_magnetic_face_halos_planned_face(
+    const gamera_cs_halo_plan *plan,
+    const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT], int receiver);
+/* cubedsphere/cubedsphere_halo.h:68-71, :84-87: unplanned fills; the device
+ * plan of the grid is built on first use and shared with the step. */
+int gamera_cs_fill_tangential_cell_halos(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                         gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                         const size_t active[3], size_t ghost);
+int gamera_cs_fill_magnetic_face_halos(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                       gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                       const size_t active[3], size_t ghost);
+/* cubedsphere/cubedsphere_halo.h:74-79 */
+int gamera_cs_fill_radial_outflow_cells(gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                        const size_t active[3], size_t ghost);
+int gamera_cs_fill_radial_outflow_cells_face(
+    gamera_no_storage storage[GAMERA_CS_FACE_COUNT], const size_t active[3],
+    size_t ghost, int receiver);
+
+/* cubedsphere/cubedsphere_interface.h:13-37: seam syncs of the face fluxes
+ * and the signed edge-EMF means (the edge-sync plan is the device context
+ * of the grid). */
+int gamera_cs_sync_magnetic_face_flux(gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                      const size_t active[3], size_t ghost);
+int gamera_cs_sync_mhd_face_fluxes(gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                   const size_t active[3], size_t ghost);
+int gamera_cs_sync_edge_emf(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                            gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                            const size_t active[3], size_t ghost);
+typedef struct gamera_cs_edge_sync_plan gamera_cs_edge_sync_plan;
+int gamera_cs_edge_sync_plan_create(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                    const size_t active[3], size_t ghost,
+                                    gamera_cs_edge_sync_plan **out);
+void gamera_cs_edge_sync_plan_destroy(gamera_cs_edge_sync_plan *plan);
+int gamera_cs_sync_edge_emf_planned(const gamera_cs_edge_sync_plan *plan,
+                                    gamera_no_storage storage[GAMERA_CS_FACE_COUNT]);
+
 /* Ionosphere potential solves, host arrays in the reference layout
  * (theta-major, longitude contiguous), synchronous.  The constant-Pedersen
  * solve runs on the GPU; its stats count the GPU's own iterations (dot

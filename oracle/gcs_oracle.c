@@ -1160,3 +1160,31 @@ static int o_edge_emf(double vt1, double vt2, double bt1, double bt2, double jmp
 
 #include "gcs_oracle_step.inc"
 #include "gcs_oracle_mi.inc"
+
+/* Stand-alone halo fills and seam syncs of the restatement (test
+ * infrastructure: checkers of the library's stand-alone entry points). */
+int gcso_fill_cell_halos(const gcso_halo_plan *p, gamera_no_storage st[6]) {
+  if (!p || !st) return -1;
+  h_fill_cells(p, st);
+  return 0;
+}
+int gcso_fill_face_halos(const gcso_halo_plan *p, const gamera_no_grid grid[6],
+                         gamera_no_storage st[6]) {
+  if (!p || !grid || !st) return -1;
+  h_fill_faces(p, grid, st);
+  return 0;
+}
+int gcso_fill_radial_outflow(gamera_no_storage st[6], const size_t act[3], size_t g) {
+  if (!st || !act) return -1;
+  h_radial(st, act, g);
+  return 0;
+}
+int gcso_sync_faces(gamera_no_storage st[6], const size_t act[3], size_t g,
+                    int magnetic) {
+  return i_sync(st, act, g, magnetic);
+}
+int gcso_sync_edges(const gcso_edge_plan *p, gamera_no_storage st[6]) {
+  if (!p || !st) return -1;
+  i_sync_edges(p, st);
+  return 0;
+}

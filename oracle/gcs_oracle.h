@@ -54,6 +54,13 @@ int gcso_edge_plan_create(const size_t active[3], size_t ghost,
                           gcso_edge_plan **out);
 void gcso_edge_plan_destroy(gcso_edge_plan *plan);
 
+int gcso_fill_cell_halos(const gcso_halo_plan *p, gamera_no_storage st[6]);
+int gcso_fill_face_halos(const gcso_halo_plan *p, const gamera_no_grid grid[6],
+                         gamera_no_storage st[6]);
+int gcso_fill_radial_outflow(gamera_no_storage st[6], const size_t act[3], size_t g);
+int gcso_sync_faces(gamera_no_storage st[6], const size_t act[3], size_t g,
+                    int magnetic);
+int gcso_sync_edges(const gcso_edge_plan *p, gamera_no_storage st[6]);
 int gcso_advance_six(const gamera_no_grid grid[6], gamera_no_storage storage[6],
                      const size_t active[3], size_t ghost, double ratio,
                      double dt, const gamera_no_advance_options *options,

@@ -46,6 +46,20 @@ def lib():
                 ("gcso_case_local_timestep", C.c_int, [C.c_void_p, P(C.c_double)]),
                 ("gcso_case_step", C.c_int, [C.c_void_p, C.c_double, C.c_double]),
                 ("gcso_case_copy_storage", C.c_int, [C.c_void_p, C.c_void_p]),
+                ("gcso_halo_plan_create", C.c_int, [P(abi.Grid), P(C.c_size_t),
+                                                    C.c_size_t, P(C.c_void_p)]),
+                ("gcso_halo_plan_destroy", None, [C.c_void_p]),
+                ("gcso_edge_plan_create", C.c_int, [P(C.c_size_t), C.c_size_t,
+                                                    P(C.c_void_p)]),
+                ("gcso_edge_plan_destroy", None, [C.c_void_p]),
+                ("gcso_fill_cell_halos", C.c_int, [C.c_void_p, P(abi.Storage)]),
+                ("gcso_fill_face_halos", C.c_int, [C.c_void_p, P(abi.Grid),
+                                                   P(abi.Storage)]),
+                ("gcso_fill_radial_outflow", C.c_int, [P(abi.Storage), P(C.c_size_t),
+                                                       C.c_size_t]),
+                ("gcso_sync_faces", C.c_int, [P(abi.Storage), P(C.c_size_t),
+                                              C.c_size_t, C.c_int]),
+                ("gcso_sync_edges", C.c_int, [C.c_void_p, P(abi.Storage)]),
                 ("gcso_mi_apply_constant_pedersen", C.c_int,
                  [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double)]),
                 ("gcso_mi_solve_constant_pedersen", C.c_int,

@@ -471,6 +471,35 @@ def run_mi(lib, torch, device, solves):
             raise RuntimeError("drop-in MI solve failed")
         if q >= 3:
             e2e.append(e2e_ms)
+    # conductance tensor (Hall = 1.5 Pedersen): SSOR-BiCGStab, one hemisphere
+    tplan = C.c_void_p()
+    tcfg = abi.MiSolverConfig.from_buffer_copy(cs[0].config)
+    tcfg.maximum_iterations = 20000
+    if lib.gcs_mi_tensor_plan_create(C.byref(tcfg), C.byref(tplan)) != 0:
+        raise RuntimeError(lib.gcs_last_error().decode())
+    P = C.POINTER(C.c_double)
+    zero_guess = np.zeros((nt, npl))
+    ttimes, tst, tstatus = [], abi.MiSolverStats(), C.c_int()
+    for q in range(3 + solves):
+        if lib.gcs_mi_tensor_plan_upload(tplan, cs[0].fac.ctypes.data_as(P),
+                                         cs[0].pedersen.ctypes.data_as(P),
+                                         cs[0].hall.ctypes.data_as(P),
+                                         zero_guess.ctypes.data_as(P)) != 0:
+            raise RuntimeError(lib.gcs_last_error().decode())
+        flush.fill_(float(q))
+        stream = torch.cuda.current_stream(device)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        if lib.gcs_mi_tensor_solve_async(tplan, C.c_void_p(stream.cuda_stream)) != 0:
+            raise RuntimeError(lib.gcs_last_error().decode())
+        ev1.record(stream)
+        if lib.gcs_mi_tensor_results(tplan, C.byref(tst), C.byref(tstatus)) != 0 or \
+                tstatus.value != 0:
+            raise RuntimeError("MI tensor solve did not converge")
+        if q >= 3:
+            ttimes.append(ev0.elapsed_time(ev1))
+    lib.gcs_mi_tensor_plan_destroy(tplan)
     ms_one, it_one, csize = out["one"]
     ms_pair, it_pair, _ = out["pair"]
     us_iter = ms_one * 1e3 / it_one[0]
@@ -491,6 +520,10 @@ def run_mi(lib, torch, device, solves):
         "effective_gbs": eff,
         "bound": "latency (2 cluster barriers per iteration; vectors on chip)",
         "solves_timed": solves,
+        "tensor": {"operator": "Pedersen + Hall (1.5x) tensor, SSOR-BiCGStab",
+                   "ms_per_call": sorted(ttimes)[len(ttimes) // 2],
+                   "iterations": tst.iterations,
+                   "launch": "one CTA of 512 threads; SSOR sweeps as row wavefronts"},
     }
 
 

@@ -90,6 +90,16 @@ def _load(path=None):
         "gamera_mi_apply_conductance_tensor": (
             C.c_int, [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double),
                       P(C.c_double), P(C.c_double)]),
+        "gamera_mi_solve_conductance_tensor": (
+            C.c_int, [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double),
+                      P(C.c_double), P(C.c_double), P(abi.MiSolverStats)]),
+        "gcs_mi_tensor_plan_create": (C.c_int, [P(abi.MiSolverConfig), P(C.c_void_p)]),
+        "gcs_mi_tensor_plan_destroy": (None, [C.c_void_p]),
+        "gcs_mi_tensor_plan_buffers": (C.c_int, [C.c_void_p] + [P(C.c_void_p)] * 4),
+        "gcs_mi_tensor_plan_upload": (C.c_int, [C.c_void_p] + [P(C.c_double)] * 4),
+        "gcs_mi_tensor_solve_async": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "gcs_mi_tensor_results": (C.c_int, [C.c_void_p, P(abi.MiSolverStats),
+                                            P(C.c_int)]),
         "gcs_mi_plan_create": (C.c_int, [P(abi.MiSolverConfig), C.c_int,
                                          P(C.c_void_p)]),
         "gcs_mi_plan_destroy": (None, [C.c_void_p]),

@@ -148,6 +148,13 @@ int gamera_mi_solve_constant_pedersen(const gamera_mi_solver_config *config,
 int gamera_mi_apply_conductance_tensor(const gamera_mi_solver_config *config,
                                        const double *pedersen, const double *hall,
                                        const double *potential_v, double *result);
+/* nonorthogonal_mi.h:99-102.  SSOR-BiCGStab on one GPU CTA: the SSOR
+ * sweeps run as row wavefronts with the reference's per-point arithmetic;
+ * at most 512 interior colatitude rows. */
+int gamera_mi_solve_conductance_tensor(const gamera_mi_solver_config *config,
+                                       const double *fac_a_m2, const double *pedersen,
+                                       const double *hall, double *potential_v,
+                                       gamera_mi_solver_stats *stats);
 
 /* Magnetosphere-ionosphere coupling, cubedsphere/cubedsphere_mi_dipole.h.
  * The FAC curl, polar sampling and both potential solves of an update run
@@ -384,6 +391,22 @@ int gcs_context_bulk_split(const gcs_context *ctx);
  * Grids up to about 100,000 unknowns per system are supported; larger ones
  * fail at plan creation.  maximum_iterations is clamped to 1,048,576. */
 typedef struct gcs_mi_plan gcs_mi_plan;
+/* Device buffers of the tensor solve for one configuration (no reference
+ * counterpart): fill the plan's buffers (gcs_mi_tensor_plan_buffers:
+ * FAC, Pedersen, Hall, initial potential, nt x np each), launch, read the
+ * stats and status (0 converged, 1 not converged, 2 non-finite FAC). */
+typedef struct gcs_mi_tensor_plan gcs_mi_tensor_plan;
+int gcs_mi_tensor_plan_create(const gamera_mi_solver_config *config,
+                              gcs_mi_tensor_plan **plan);
+void gcs_mi_tensor_plan_destroy(gcs_mi_tensor_plan *plan);
+int gcs_mi_tensor_plan_buffers(gcs_mi_tensor_plan *plan, double **fac, double **pedersen,
+                               double **hall, double **potential);
+int gcs_mi_tensor_plan_upload(gcs_mi_tensor_plan *plan, const double *fac,
+                              const double *pedersen, const double *hall,
+                              const double *potential);
+int gcs_mi_tensor_solve_async(gcs_mi_tensor_plan *plan, void *stream);
+int gcs_mi_tensor_results(gcs_mi_tensor_plan *plan, gamera_mi_solver_stats *stats,
+                          int *status);
 /* Ionosphere coupling of a device-built case (gcs_context_create_case with
  * a background): as gamera_cs_mi_dipole_create, with the state, geometry
  * and B0 taken from the context; the shell must lie within the innermost

@@ -1,0 +1,109 @@
+"""The CUDA conductance-tensor solve (SSOR-BiCGStab) against the
+reference.  The BiCGStab dot products are summed in a fixed parallel order,
+so iterates differ from the CPU solver's at rounding level; a solve passes
+when it converges, its true residual -- evaluated on the CPU with the
+oracle's tensor operator -- meets the reference target (slack 1e-9), its
+potential is within 5e-8 of max|potential| of the reference's and its
+iteration count within 10 % (at least 3)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mi_util import POTENTIAL_RTOL, golden, golden_case, ptr
+from oracle import oracle_cases
+
+pytestmark = pytest.mark.gpu
+
+
+def glib():
+    import gamera_cube_b200
+    return gamera_cube_b200.lib
+
+
+def tensor_residual(cfg, fac, sp, sh, pot):
+    npl, nt = cfg.longitude_count, cfg.colatitude_count
+    ap = np.zeros_like(pot)
+    assert oracle_cases.lib().gcso_mi_apply_conductance_tensor(
+        C.byref(cfg), ptr(sp), ptr(sh), ptr(pot), ptr(ap)) == 0
+    dth = cfg.maximum_colatitude / (nt - 1)
+    th = dth * np.arange(1, nt - 1)
+    c = np.cos(th)
+    inc = cfg.hemisphere * 2.0 * c / np.sqrt(1.0 + 3.0 * c * c)
+    u = -(cfg.ionosphere_radius_m ** 2) * fac[1:nt - 1] * inc[:, None]
+    res = u - ap[1:nt - 1]
+    # pole row: the reduced system's pole equation, scaled like the reference norm
+    norm2 = npl * ap[0, 0] ** 2 + np.sum(res * res)
+    target = max(cfg.absolute_tolerance,
+                 cfg.relative_tolerance * max(np.sqrt(np.sum(u * u)), 1.0))
+    return float(np.sqrt(norm2)), float(target)
+
+
+def solve(lib, fn, cfg, d, guess):
+    from gamera_cube_b200 import abi
+    pot = guess.copy()
+    st = abi.MiSolverStats()
+    rc = fn(C.byref(cfg), ptr(d["fac"]), ptr(d["pedersen"]), ptr(d["hall"]), ptr(pot),
+            C.byref(st))
+    return rc, pot, st
+
+
+def check(cfg, d, pot, st, ref_pot, ref_iters):
+    assert st.converged == 1
+    scale = np.abs(ref_pot).max()
+    assert np.abs(pot - ref_pot).max() <= POTENTIAL_RTOL * scale
+    assert abs(st.iterations - ref_iters) <= max(3, 0.1 * ref_iters)
+    assert np.all(pot[0] == pot[0, 0]) and np.all(pot[-1] == 0.0)
+
+
+@pytest.mark.parametrize("name", ["small_north", "shell_192x22"])
+def test_tensor_against_golden(name):
+    g = golden()
+    cfg, d = golden_case(g, name, tensor=True)
+    rc, pot, st = solve(glib(), glib().gamera_mi_solve_conductance_tensor, cfg, d,
+                        d["guess"])
+    assert rc == 0
+    check(cfg, d, pot, st, g[name + "/tensor/potential"],
+          int(g[name + "/tensor/stats"][0]))
+    assert st.initial_residual == pytest.approx(g[name + "/tensor/stats"][1], rel=1e-12)
+
+
+def test_tensor_production_grid():
+    """181 x 361, Hall = 1.5 Pedersen, against the oracle."""
+    from gamera_cube_b200 import cases
+    case = cases.mi_case(361, 181, seed=21, max_iterations=20000)
+    d = {"fac": case.fac, "pedersen": case.pedersen, "hall": case.hall}
+    O = oracle_cases.lib()
+    rc, ref_pot, ref_st = solve(O, O.gcso_mi_solve_conductance_tensor, case.config, d,
+                                case.potential)
+    assert rc == 0
+    rc, pot, st = solve(glib(), glib().gamera_mi_solve_conductance_tensor, case.config,
+                        d, case.potential)
+    assert rc == 0
+    check(case.config, d, pot, st, ref_pot, ref_st.iterations)
+
+
+def test_tensor_rejects_bad_input():
+    from gamera_cube_b200 import abi, cases
+    L = glib()
+    case = cases.mi_case(24, 12, seed=3)
+    d = {"fac": case.fac.copy(), "pedersen": case.pedersen.copy(),
+         "hall": case.hall.copy()}
+    d["fac"][4, 5] = np.nan
+    pot = np.full_like(case.fac, 2.0)
+    st = abi.MiSolverStats()
+    st.iterations = -3
+    assert L.gamera_mi_solve_conductance_tensor(
+        C.byref(case.config), ptr(d["fac"]), ptr(d["pedersen"]), ptr(d["hall"]),
+        ptr(pot), C.byref(st)) == -1
+    assert np.all(pot == 2.0) and st.iterations == -3
+    d["fac"][4, 5] = 0.0
+    d["pedersen"][0, 0] = -1.0
+    assert L.gamera_mi_solve_conductance_tensor(
+        C.byref(case.config), ptr(d["fac"]), ptr(d["pedersen"]), ptr(d["hall"]),
+        ptr(pot), C.byref(st)) == -1
+    d["pedersen"][0, 0] = 1.0
+    bad = cases.mi_config(24, 12, low_latitude_potential_v=3.0)
+    assert L.gamera_mi_solve_conductance_tensor(
+        C.byref(bad), ptr(d["fac"]), ptr(d["pedersen"]), ptr(d["hall"]), ptr(pot),
+        C.byref(st)) == -1

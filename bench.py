@@ -523,7 +523,7 @@ def run_mi(lib, torch, device, solves):
         "tensor": {"operator": "Pedersen + Hall (1.5x) tensor, SSOR-BiCGStab",
                    "ms_per_call": sorted(ttimes)[len(ttimes) // 2],
                    "iterations": tst.iterations,
-                   "launch": "one CTA of 512 threads; SSOR sweeps as row wavefronts"},
+                   "launch": "one thread-block cluster (16 CTAs); SSOR sweeps by one warp along anti-diagonals, diagonals moved by bulk async copies"},
     }
 
 

@@ -111,6 +111,18 @@ def _load(path=None):
             C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "gcs_mi_plan_results": (C.c_int, [C.c_void_p, P(abi.MiSolverStats),
                                           P(C.c_int)]),
+        "gcs_mi_net_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint,
+                                        P(C.c_void_p)]),
+        "gcs_mi_net_destroy": (None, [C.c_void_p]),
+        "gcs_mi_net_info": (C.c_int, [C.c_void_p] + [P(C.c_int)] * 4),
+        "gcs_mi_net_get_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int, C.c_int]),
+        "gcs_mi_net_set_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int]),
+        "gcs_mi_net_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+        "gcs_mi_net_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                            C.c_float, C.c_int, P(C.c_float)]),
+        "gcs_mi_solve_conductance_tensor_learned": (
+            C.c_int, [C.c_void_p, P(abi.MiSolverConfig)] + [P(C.c_double)] * 4 +
+            [P(abi.MiSolverStats), P(C.c_int)]),
     }
     sig["gcs_context_set_precision"] = (C.c_int, [C.c_void_p, C.c_int])
     sig["gcs_context_precision"] = (C.c_int, [C.c_void_p])

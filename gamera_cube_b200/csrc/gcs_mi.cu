@@ -854,10 +854,16 @@ struct Shape {
   size_t smem = 0;
 };
 
+// Dynamic shared memory of any launch shape (launchable rejects more).
+constexpr size_t kShapeSmemCap = 200 * 1024;
+
+// The kernel's shared-memory limit is set to the cap, not to this shape's
+// need, so configuring a shape for a small grid never lowers it under a
+// shape chosen earlier for a larger one.
 cudaError_t configure(const Shape &sh) {
   cudaError_t e = cudaFuncSetAttribute(sh.kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sh.smem);
+                                       (int)kShapeSmemCap);
   if (e != cudaSuccess) return e;
   if (sh.csize > kPortableCluster)
     e = cudaFuncSetAttribute(sh.kernel, cudaFuncAttributeNonPortableClusterSizeAllowed,
@@ -882,7 +888,7 @@ cudaLaunchConfig_t launch_config(const Shape &sh, int count, cudaStream_t stream
 }
 
 bool launchable(const Shape &sh) {
-  if (sh.smem > 200 * 1024 || configure(sh) != cudaSuccess) {
+  if (sh.smem > kShapeSmemCap || configure(sh) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -918,7 +924,7 @@ size_t band_smem(int rows, int np) {
          (size_t)rows * sizeof(Row);
 }
 
-constexpr size_t kMaxSmem = 200 * 1024;
+constexpr size_t kMaxSmem = kShapeSmemCap;
 
 }  // namespace mi
 }  // namespace gcs

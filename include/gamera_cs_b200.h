@@ -425,6 +425,42 @@ int gcs_mi_solve_constant_pedersen_async(gcs_mi_plan *plan, const double *fac,
 int gcs_mi_plan_results(gcs_mi_plan *plan, gamera_mi_solver_stats *stats,
                         int *status);
 
+/* Learned preconditioner of the conductance-tensor ionosphere solve (no
+ * reference counterpart): a four-level convolutional network on the polar
+ * grid (interior rows x longitudes, padded to H0 x W0: gcs_mi_net_info), BF16
+ * weights and activations with FP32 accumulation on the tensor cores.
+ * Inputs [B][4][H0][W0] and outputs / targets [B][H0][W0] are FP32 device
+ * arrays.  Parameters are exchanged packed: per convolution and output
+ * channel, 9 x input-channel weights then the bias (gradients = 1 returns
+ * the gradients of the last training step instead). */
+typedef struct gcs_mi_net gcs_mi_net;
+int gcs_mi_net_create(int interior_rows, int longitudes, int max_batch, unsigned seed,
+                      gcs_mi_net **net);
+void gcs_mi_net_destroy(gcs_mi_net *net);
+int gcs_mi_net_info(const gcs_mi_net *net, int *H0, int *W0, int *params,
+                    int *in_channels);
+int gcs_mi_net_get_params(gcs_mi_net *net, float *params, int count, int gradients);
+int gcs_mi_net_set_params(gcs_mi_net *net, const float *params, int count);
+int gcs_mi_net_forward(gcs_mi_net *net, const float *inputs, int batch, float *outputs);
+/* Loss sum over valid points of (output - target)^2 / (batch x rows x
+ * longitudes) and its gradients; update != 0 applies one Adam step. */
+int gcs_mi_net_train_step(gcs_mi_net *net, const float *inputs, const float *targets,
+                          int batch, float learning_rate, int update, float *loss);
+/* The conductance-tensor solve (arguments, validation and result as
+ * gamera_mi_solve_conductance_tensor, nonorthogonal_mi.h:96-102) by flexible
+ * GMRES(40) on the reduced system with its rows scaled so that the residual
+ * 2-norm is the reference's residual norm, preconditioned by the network
+ * (net, built for interior_rows = colatitude_count - 2 and longitudes =
+ * longitude_count) or by Jacobi (net = NULL).  Convergence is judged on the
+ * FP64 true residual against the reference's target.  If maximum_iterations
+ * pass without convergence, the reference algorithm continues from the
+ * iterate and *fallback is set to 1.  No reference counterpart. */
+int gcs_mi_solve_conductance_tensor_learned(gcs_mi_net *net,
+                                            const gamera_mi_solver_config *config,
+                                            const double *fac_a_m2, const double *pedersen,
+                                            const double *hall, double *potential_v,
+                                            gamera_mi_solver_stats *stats, int *fallback);
+
 #ifdef __cplusplus
 }
 #endif

@@ -228,3 +228,41 @@ def test_launch_shapes(npl, nt, threads):
     ref = oracle_solve(case.config, case.fac, case.potential)
     assert ref[0] == 0
     check_solution(case.config, case.fac, pot, st, ref[1], ref[2].iterations)
+
+
+def test_plans_of_different_widths_coexist():
+    """A plan made for a narrow grid must not stop an earlier plan for a
+    wider grid (same kernel, more shared memory) from launching."""
+    from gamera_cube_b200 import abi, cases
+    L = glib()
+    wide = cases.mi_case(361, 22, seed=5)
+    narrow = cases.mi_case(64, 22, seed=6)
+    plans = []
+    try:
+        for case in (wide, narrow):
+            plan = C.c_void_p()
+            assert L.gcs_mi_plan_create(C.byref(case.config), 1, C.byref(plan)) == 0
+            plans.append(plan)
+        smem = [C.c_size_t(), C.c_size_t()]
+        for plan, s in zip(plans, smem):
+            L.gcs_mi_plan_info(plan, None, None, C.byref(s))
+        assert smem[0].value > smem[1].value
+        import torch
+        fac_d = torch.from_numpy(wide.fac.ravel()).cuda()
+        pot_d = torch.from_numpy(wide.potential.ravel()).cuda()
+        torch.cuda.synchronize()
+        assert L.gcs_mi_solve_constant_pedersen_async(
+            plans[0], C.c_void_p(fac_d.data_ptr()), C.c_void_p(pot_d.data_ptr()),
+            None) == 0, L.gcs_last_error().decode()
+        stats = (abi.MiSolverStats * 1)()
+        status = (C.c_int * 1)()
+        assert L.gcs_mi_plan_results(plans[0], stats, status) == 0, \
+            L.gcs_last_error().decode()
+        assert status[0] == 0
+        pot = pot_d.cpu().numpy().reshape(22, 361)
+    finally:
+        for plan in plans:
+            L.gcs_mi_plan_destroy(plan)
+    rc, ref_pot, ref_st = oracle_solve(wide.config, wide.fac, wide.potential)
+    assert rc == 0
+    check_solution(wide.config, wide.fac, pot, stats[0], ref_pot, ref_st.iterations)

@@ -500,6 +500,7 @@ def run_mi(lib, torch, device, solves):
         if q >= 3:
             ttimes.append(ev0.elapsed_time(ev1))
     lib.gcs_mi_tensor_plan_destroy(tplan)
+    two_level, learned = mi_flexible(lib, cs[0], solves)
     ms_one, it_one, csize = out["one"]
     ms_pair, it_pair, _ = out["pair"]
     us_iter = ms_one * 1e3 / it_one[0]
@@ -524,7 +525,53 @@ def run_mi(lib, torch, device, solves):
                    "ms_per_call": sorted(ttimes)[len(ttimes) // 2],
                    "iterations": tst.iterations,
                    "launch": "one thread-block cluster (16 CTAs); SSOR sweeps by one warp along anti-diagonals, diagonals moved by bulk async copies"},
+        "tensor_two_level": two_level,
+        "tensor_learned": learned,
     }
+
+
+def mi_flexible(lib, case, solves, train_steps=600):
+    """The conductance-tensor case by flexible GMRES: left two-level
+    preconditioner (ring-mean coarse correction + damped Jacobi) alone, and
+    with the learned network as the right preconditioner after a short
+    training on the GPU (random potentials and solved R1/R2 cases on the
+    seeded production conductances).  Host arrays, synchronous calls, wall
+    clock (the solve reads one Hessenberg column per iteration)."""
+    import numpy as np
+    from gamera_cube_b200 import cases, learn
+    tcase = cases.mi_case(case.config.longitude_count, case.config.colatitude_count, seed=7,
+                          max_iterations=3000)
+    runs = []
+    for q in range(2 + solves):
+        rc, _, st, fb, sec = learn.solve(lib, None, tcase, method=2)
+        if rc != 0 or fb:
+            raise RuntimeError("two-level MI solve failed")
+        if q >= 2:
+            runs.append(sec * 1e3)
+    two_level = {"operator": "Pedersen + Hall (1.5x) tensor, flexible GMRES(40), left "
+                             "two-level preconditioner (ring-mean coarse correction, 2 damped "
+                             "Jacobi steps)",
+                 "ms_per_call": sorted(runs)[len(runs) // 2], "iterations": st.iterations}
+    t0 = time.perf_counter()
+    net = learn.create_net(lib, tcase.config, batch=8, seed=3)
+    try:
+        pool = learn.Pool(lib, npl=tcase.config.longitude_count,
+                          nt=tcase.config.colatitude_count, random_fields=128, solved=4,
+                          conductances=8)
+        losses = learn.train(lib, net, pool, steps=train_steps, batch=8, lr=1e-3)
+        train_s = time.perf_counter() - t0
+        rc, _, st, fb, sec = learn.solve(lib, net, tcase, method=0)
+        rc, _, st, fb, sec = learn.solve(lib, net, tcase, method=0)
+    finally:
+        lib.gcs_mi_net_destroy(net)
+    learned = {"operator": "as tensor_two_level with the BF16 conv net (194,769 parameters) as "
+                           "the flexible right preconditioner",
+               "training": {"steps": train_steps, "batch": 8, "triples": pool.triples,
+                            "seconds": train_s, "loss_first": float(losses[0]),
+                            "loss_last": float(np.mean(losses[-20:]))},
+               "ms_per_call": sec * 1e3, "iterations": st.iterations,
+               "fell_back_to_reference_algorithm": bool(fb), "converged": rc == 0}
+    return two_level, learned
 
 
 def mi_cpu_baseline():

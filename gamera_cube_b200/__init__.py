@@ -121,8 +121,10 @@ def _load(path=None):
         "gcs_mi_net_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                             C.c_float, C.c_int, P(C.c_float)]),
         "gcs_mi_solve_conductance_tensor_learned": (
-            C.c_int, [C.c_void_p, P(abi.MiSolverConfig)] + [P(C.c_double)] * 4 +
+            C.c_int, [C.c_void_p, C.c_int, P(abi.MiSolverConfig)] + [P(C.c_double)] * 4 +
             [P(abi.MiSolverStats), P(C.c_int)]),
+        "gcs_mi_learned_apply": (C.c_int, [C.c_void_p, C.c_int, C.c_int,
+                                           P(abi.MiSolverConfig)] + [P(C.c_double)] * 4),
     }
     sig["gcs_context_set_precision"] = (C.c_int, [C.c_void_p, C.c_int])
     sig["gcs_context_precision"] = (C.c_int, [C.c_void_p])

@@ -517,7 +517,12 @@ struct LpSys {
   double *pe, *dg0;                   // np, 1
   double *scale;                      // n: row scale of the reduced system
   double *b, *x;                      // n: scaled right-hand side, iterate
+  // ring coarse operator T = E^T A' E (E: one value per colatitude ring and
+  // the pole), tridiagonal; Thomas factors
+  double *tl, *td, *tu, *cp, *cm;     // R + 1 each
 };
+
+constexpr int kMaxRingRows = 2048;    // ring rows of the one-block ring solve
 
 // Coefficients (nonorthogonal_mi.c:776-865), scaled right-hand side and the
 // initial guess (:999-1029) of the reduced system.
@@ -684,7 +689,9 @@ __global__ void k_lp_update(double *x, const double *Z, size_t n, int cnt, const
 // Network input channel 0 from a unit-norm Krylov vector: unit RMS over
 // the interior, periodic continuation in the padding columns, zero rows
 // below; channels 1-3 are the fixed features.
-__global__ void k_lp_pack(const double *v, float *in, int R, int np, int H0, int W0, double s) {
+__global__ void k_lp_pack(const double *v, float *in, int R, int np, int H0, int W0,
+                          const double *nrm2, double count) {
+  const double s = sqrt(count / *nrm2);
   const size_t n = (size_t)H0 * W0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
@@ -695,21 +702,23 @@ __global__ void k_lp_pack(const double *v, float *in, int R, int np, int H0, int
 
 // Z_k from the network output: interior points, the pole the mean of the
 // first interior row.  One block.
-__global__ void k_lp_unpack(const float *out, double *z, int R, int np, int W0) {
+__global__ void k_lp_unpack(const float *out, double *z, int R, int np, int W0,
+                            const double *nrm2, double count) {
   __shared__ double part[32];
+  const double s = sqrt(*nrm2 / count);  // the network's output is in units of the input RMS
   double a = 0.0;
   for (int j = threadIdx.x; j < np; j += blockDim.x) a += out[j];
   for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
   if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = a;
   for (size_t q = threadIdx.x; q < (size_t)R * np; q += blockDim.x) {
     const int h = (int)(q / np), w = (int)(q - (size_t)h * np);
-    z[1 + q] = out[(size_t)h * W0 + w];
+    z[1 + q] += s * out[(size_t)h * W0 + w];
   }
   __syncthreads();
   if (threadIdx.x < 32) {
     a = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (threadIdx.x == 0) z[0] = a / (double)np;
+    if (threadIdx.x == 0) z[0] += s * a / (double)np;
   }
 }
 
@@ -719,6 +728,108 @@ __global__ void k_lp_jacobi(const LpSys S, const double *v, double *z) {
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q <= nq;
        q += (size_t)gridDim.x * blockDim.x)
     z[q] = q == 0 ? v[0] * S.scale[0] / *S.dg0 : v[q] * S.scale[q] / S.dg[q - 1];
+}
+
+// z += omega D'^-1 r (damped Jacobi step of the scaled system)
+__global__ void k_lp_jacobi_add(const LpSys S, const double *r, double *z, double omega) {
+  const size_t nq = (size_t)S.R * S.np;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q <= nq;
+       q += (size_t)gridDim.x * blockDim.x)
+    z[q] += omega * (q == 0 ? r[0] * S.scale[0] / *S.dg0 : r[q] * S.scale[q] / S.dg[q - 1]);
+}
+
+// Ring coarse operator: row 0 the pole, row i >= 1 interior row i - 1 with
+// its coefficients summed over longitude (the Hall terms cancel in the
+// sums around a ring).  One block per coarse row.
+__global__ void k_lp_ring_setup(LpSys S) {
+  const int i = blockIdx.x, np = S.np;
+  __shared__ double part[3][32];
+  double a = 0.0, l = 0.0, u = 0.0;
+  if (i == 0) {
+    for (int j = threadIdx.x; j < np; j += blockDim.x) a += S.pe[j];
+  } else {
+    const int row = i - 1;
+    for (int j = threadIdx.x; j < np; j += blockDim.x) {
+      const size_t q = (size_t)row * np + j;
+      a += S.dg[q] + S.ll[q] + S.lu[q];
+      l += S.lo[q];
+      u += S.up[q];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    l += __shfl_xor_sync(0xffffffffu, l, o);
+    u += __shfl_xor_sync(0xffffffffu, u, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    part[0][threadIdx.x >> 5] = a;
+    part[1][threadIdx.x >> 5] = l;
+    part[2][threadIdx.x >> 5] = u;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = l = u = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += part[0][w];
+      l += part[1][w];
+      u += part[2][w];
+    }
+    if (i == 0) {
+      S.td[0] = *S.dg0 / S.scale[0];
+      S.tl[0] = 0.0;
+      S.tu[0] = -a / S.scale[0];
+    } else {
+      const double s = S.row_s[i];
+      S.td[i] = a / s;
+      S.tl[i] = l / s;
+      S.tu[i] = i < S.R ? u / s : 0.0;
+    }
+  }
+}
+
+// Thomas factors of the ring operator (one thread).
+__global__ void k_lp_ring_factor(LpSys S) {
+  double prev = 0.0;
+  for (int i = 0; i <= S.R; ++i) {
+    const double m = S.td[i] - S.tl[i] * prev;
+    S.cm[i] = 1.0 / m;
+    prev = S.tu[i] / m;
+    S.cp[i] = prev;
+  }
+}
+
+// z (+)= E T^-1 E^T r: ring sums, the tridiagonal solve, prolongation.
+// One block.
+__global__ void __launch_bounds__(1024) k_lp_ring_solve(const LpSys S, const double *r,
+                                                        double *z, int accumulate) {
+  __shared__ double c[kMaxRingRows + 1];
+  const int np = S.np, R = S.R, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  for (int i = warp; i <= R; i += nw) {
+    double a = 0.0;
+    if (i == 0) {
+      a = lane == 0 ? r[0] : 0.0;
+    } else {
+      for (int j = lane; j < np; j += 32) a += r[1 + (size_t)(i - 1) * np + j];
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) c[i] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double prev = 0.0;
+    for (int i = 0; i <= R; ++i) {
+      prev = (c[i] - S.tl[i] * prev) * S.cm[i];
+      c[i] = prev;
+    }
+    for (int i = R - 1; i >= 0; --i) c[i] -= S.cp[i] * c[i + 1];
+  }
+  __syncthreads();
+  const size_t n = 1 + (size_t)R * np;
+  for (size_t q = threadIdx.x; q < n; q += blockDim.x) {
+    const double v = q == 0 ? c[0] : c[1 + (q - 1) / np];
+    z[q] = accumulate ? z[q] + v : v;
+  }
 }
 
 // Network feature channels 1-3: log(Sigma_P / 5 S), Sigma_H / Sigma_P,
@@ -778,7 +889,7 @@ struct gcs_mi_learned_plan {
   void *pool = nullptr;
   double *V = nullptr, *Z = nullptr, *w = nullptr, *part = nullptr, *h = nullptr,
          *hy = nullptr, *nrm = nullptr, *pot = nullptr, *fac = nullptr, *sp = nullptr,
-         *sh = nullptr;
+         *sh = nullptr, *r = nullptr, *t = nullptr, *rn = nullptr;
   float *net_in = nullptr, *net_out = nullptr;
   double *host = nullptr;  // pinned: the last Hessenberg column and norms
 };
@@ -794,6 +905,7 @@ void lp_free(gcs_mi_learned_plan *p) {
 
 gcs_mi_learned_plan *lp_create(const gamera_mi_solver_config *c, const gcs_mi_net *net) {
   if (!c || c->colatitude_count < 3U || c->longitude_count < 4U ||
+      c->colatitude_count - 2U > (unsigned)kMaxRingRows ||
       (net && (net->R != (int)c->colatitude_count - 2 || net->np != (int)c->longitude_count))) {
     set_api_error("learned MI solve: network grid and configuration differ");
     return nullptr;
@@ -806,7 +918,8 @@ gcs_mi_learned_plan *lp_create(const gamera_mi_solver_config *c, const gcs_mi_ne
   p->n = 1 + (size_t)p->R * p->np;
   const size_t nodes = (size_t)p->np * p->nt, nq = (size_t)p->R * p->np, n = p->n;
   const int H0 = round_up(p->R, 8), W0 = round_up(p->np, 32);
-  const size_t doubles = 5 * nq + p->np + 8 + 3 * n + (2 * (size_t)kRestartLen + 2) * n +
+  const size_t doubles = 5 * nq + p->np + 8 + 5 * n + (2 * (size_t)kRestartLen + 2) * n +
+                         5 * ((size_t)p->R + 1 + 32) + 16 +
                          (size_t)kDotBlocks * (kRestartLen + 2) + 2 * (kRestartLen + 2) +
                          4 * nodes + 6 * (size_t)p->nt;
   const size_t floats = 5 * (size_t)H0 * W0;
@@ -830,6 +943,14 @@ gcs_mi_learned_plan *lp_create(const gamera_mi_solver_config *c, const gcs_mi_ne
   S.ll = take(nq);
   S.lu = take(nq);
   S.pe = take(p->np);
+  S.tl = take(p->R + 1);
+  S.td = take(p->R + 1);
+  S.tu = take(p->R + 1);
+  S.cp = take(p->R + 1);
+  S.cm = take(p->R + 1);
+  p->r = take(n);
+  p->t = take(n);
+  p->rn = take(8);
   S.dg0 = take(8);
   S.scale = take(n);
   S.b = take(n);
@@ -903,16 +1024,65 @@ void lp_dots(gcs_mi_learned_plan *p, const double *w, int cnt, int norm, double 
                                          accumulate);
 }
 
-// Flexible GMRES with the network (net) or Jacobi (net == NULL) as the
-// preconditioner; returns 0 converged, 1 not converged, -1 error.
-int lp_solve(gcs_mi_learned_plan *p, gcs_mi_net *net, gamera_mi_solver_stats *st) {
+// out = L v, the left preconditioner: Jacobi (method 1) or the two-level
+// step (methods 0 and 2): a coarse correction on ring means, E T^-1 E^T
+// (one value per colatitude ring and the pole), two damped Jacobi steps and
+// the coarse correction again, each on the current residual.  Linear.
+// Uses p->r.
+void lp_left(gcs_mi_learned_plan *p, int method, const double *v, double *z) {
+  LpSys &S = p->S;
+  const unsigned nb = lp_blocks(p->n);
+  if (method == 1) {
+    k_lp_jacobi<<<nb, 256>>>(S, v, z);
+    return;
+  }
+  const int ring_threads = 1024;
+  k_lp_ring_solve<<<1, ring_threads>>>(S, v, z, 0);
+  k_lp_apply<<<nb, 256>>>(S, z, p->r, v);
+  k_lp_jacobi_add<<<nb, 256>>>(S, p->r, z, 0.7);
+  k_lp_apply<<<nb, 256>>>(S, z, p->r, v);
+  k_lp_jacobi_add<<<nb, 256>>>(S, p->r, z, 0.7);
+  k_lp_apply<<<nb, 256>>>(S, z, p->r, v);
+  k_lp_ring_solve<<<1, ring_threads>>>(S, p->r, z, 1);
+}
+
+// z = N v, the flexible right preconditioner: the network (method 0) on v
+// at unit RMS, its output in units of that RMS; the identity otherwise.
+bool lp_right(gcs_mi_learned_plan *p, gcs_mi_net *net, int method, const double *v,
+              double *z) {
+  const size_t n = p->n;
+  if (method != 0)
+    return cuda_ok(cudaMemcpyAsync(z, v, n * sizeof(double), cudaMemcpyDeviceToDevice),
+                   "cudaMemcpyAsync");
+  const int H0 = round_up(p->R, 8), W0 = round_up(p->np, 32);
+  lp_dots(p, v, 0, 1, p->rn, 0);
+  k_lp_pack<<<lp_blocks((size_t)H0 * W0), 256>>>(v, p->net_in, p->R, p->np, H0, W0, p->rn,
+                                                 (double)n);
+  if (gcs_mi_net_forward(net, p->net_in, 1, nullptr) != 0) return false;
+  if (!cuda_ok(cudaMemsetAsync(z, 0, n * sizeof(double)), "cudaMemsetAsync")) return false;
+  k_lp_unpack<<<1, 256>>>(net->out32, z, p->R, p->np, W0, p->rn, (double)n);
+  return true;
+}
+
+// Flexible GMRES(40) on L A x = L b with the right preconditioner N
+// (methods: 0 two-level L and the network N, 1 Jacobi L, 2 two-level L and
+// N = I).  The left factor is linear, so the Krylov space is that of the
+// well-conditioned L A; the inner iteration stops at a reduction of |L r|
+// proportional to the true reduction still needed, and every restart
+// recomputes the true residual |b - A x| (the reference's norm) and judges
+// convergence on it.  Returns 0 converged, 1 not converged, -1 error.
+int lp_solve(gcs_mi_learned_plan *p, gcs_mi_net *net, int method, gamera_mi_solver_stats *st) {
   LpSys &S = p->S;
   const size_t n = p->n;
   const unsigned nb = lp_blocks(n);
   const int H0 = round_up(p->R, 8), W0 = round_up(p->np, 32);
   k_lp_setup<<<lp_blocks((size_t)p->R * p->np), 256>>>(S);
   k_lp_dg0<<<1, 32>>>(S);
-  if (net) k_lp_features<<<lp_blocks((size_t)H0 * W0), 256>>>(S, p->net_in, H0, W0);
+  if (method != 1) {
+    k_lp_ring_setup<<<p->R + 1, 256>>>(S);
+    k_lp_ring_factor<<<1, 1>>>(S);
+  }
+  if (method == 0) k_lp_features<<<lp_blocks((size_t)H0 * W0), 256>>>(S, p->net_in, H0, W0);
   double *hh = p->host;
   // target from |u| = |b| (scaled right-hand side, interior only: b[0] = 0)
   k_lp_dots<<<kDotBlocks, 256>>>(S.b, p->V, n, 0, 1, p->part);
@@ -928,31 +1098,30 @@ int lp_solve(gcs_mi_learned_plan *p, gcs_mi_net *net, gamera_mi_solver_stats *st
   int iters = 0;
   double initial = -1.0, res = 0.0;
   for (;;) {
-    // true residual r = b - A x into V_0, |r|^2
-    k_lp_apply<<<nb, 256>>>(S, S.x, p->V, S.b);
-    k_lp_dots<<<kDotBlocks, 256>>>(p->V, p->V, n, 0, 1, p->part);
-    k_lp_sum<<<1, 32>>>(p->part, kDotBlocks, 1, p->h, 0);
-    if (!cuda_ok(cudaMemcpy(hh, p->h, sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy"))
+    // true residual r = b - A x, |r|^2; s = L r into V_0, |s|^2
+    k_lp_apply<<<nb, 256>>>(S, S.x, p->t, S.b);
+    lp_dots(p, p->t, 0, 1, p->h, 0);
+    lp_left(p, method, p->t, p->V);
+    lp_dots(p, p->V, 0, 1, p->h + 1, 0);
+    if (!cuda_ok(cudaMemcpy(hh, p->h, 2 * sizeof(double), cudaMemcpyDeviceToHost),
+                 "cudaMemcpy"))
       return -1;
     res = sqrt(fmax(0.0, hh[0]));
+    const double beta = sqrt(fmax(0.0, hh[1]));
     if (initial < 0.0) initial = res;
-    if (!std::isfinite(res)) return -1;
-    if (res <= target || iters >= max_iter) break;
-    k_lp_normalise<<<nb, 256>>>(p->V, p->V, n, p->h);
+    if (!std::isfinite(res) || !std::isfinite(beta)) return -1;
+    if (res <= target || iters >= max_iter || !(beta > 0.0)) break;
+    // |L r| reduction matching the true reduction still needed, with margin
+    const double inner = 0.3 * beta * target / res;
+    k_lp_normalise<<<nb, 256>>>(p->V, p->V, n, p->h + 1);
     std::fill(g.begin(), g.end(), 0.0);
-    g[0] = res;
+    g[0] = beta;
     int j = 0;
     for (; j < kRestartLen && iters < max_iter; ++j) {
       double *vj = p->V + (size_t)j * n, *zj = p->Z + (size_t)j * n;
-      if (net) {
-        k_lp_pack<<<lp_blocks((size_t)H0 * W0), 256>>>(vj, p->net_in, p->R, p->np, H0, W0,
-                                                       sqrt((double)n));
-        if (gcs_mi_net_forward(net, p->net_in, 1, nullptr) != 0) return -1;
-        k_lp_unpack<<<1, 256>>>(net->out32, zj, p->R, p->np, W0);
-      } else {
-        k_lp_jacobi<<<nb, 256>>>(S, vj, zj);
-      }
-      k_lp_apply<<<nb, 256>>>(S, zj, p->w, nullptr);
+      if (!lp_right(p, net, method, vj, zj)) return -1;
+      k_lp_apply<<<nb, 256>>>(S, zj, p->t, nullptr);
+      lp_left(p, method, p->t, p->w);
       // classical Gram-Schmidt, twice; then |w|^2
       lp_dots(p, p->w, j + 1, 0, p->h, 0);
       k_lp_orth<<<nb, 256>>>(p->w, p->V, n, j + 1, p->h);
@@ -985,7 +1154,7 @@ int lp_solve(gcs_mi_learned_plan *p, gcs_mi_net *net, gamera_mi_solver_stats *st
       col[j + 1] = 0.0;
       g[j + 1] = -sn[j] * g[j];
       g[j] = cs[j] * g[j];
-      if (!(hn > 0.0) || fabs(g[j + 1]) <= 0.5 * target) {
+      if (!(hn > 0.0) || fabs(g[j + 1]) <= inner) {
         ++j;
         break;
       }
@@ -1014,18 +1183,22 @@ gcs_mi_learned_plan *g_lp_cache = nullptr;
 
 extern "C" {
 
-// Conductance-tensor solve (host arrays, synchronous) by flexible GMRES
-// preconditioned with the network (net) or, net == NULL, by Jacobi.  When
+// Conductance-tensor solve (host arrays, synchronous) by lp_solve's method
+// (0 needs the network).  When
 // the iteration limit is reached without convergence the reference
 // algorithm (gamera_mi_solve_conductance_tensor) continues from the
 // iterate; *fallback reports it.  Same arguments, validation and result
 // convention as gamera_mi_solve_conductance_tensor.
-int gcs_mi_solve_conductance_tensor_learned(gcs_mi_net *net,
+int gcs_mi_solve_conductance_tensor_learned(gcs_mi_net *net, int method,
                                             const gamera_mi_solver_config *config,
                                             const double *fac_a_m2, const double *pedersen,
                                             const double *hall, double *potential_v,
                                             gamera_mi_solver_stats *stats, int *fallback) {
   if (fallback) *fallback = 0;
+  if (method < 0 || method > 2 || (method == 0 && !net)) {
+    set_api_error("learned MI solve: method 0 needs a network, methods are 0, 1, 2");
+    return -1;
+  }
   if (!config || !fac_a_m2 || !pedersen || !hall || !potential_v || config->maximum_iterations <= 0 ||
       !(config->relative_tolerance > 0.0) || config->colatitude_count < 3U ||
       config->longitude_count < 4U) {
@@ -1060,7 +1233,7 @@ int gcs_mi_solve_conductance_tensor_learned(gcs_mi_net *net,
       !cuda_ok(cudaMemcpy(p->pot, potential_v, bytes, cudaMemcpyHostToDevice), "cudaMemcpy"))
     return -1;
   gamera_mi_solver_stats s{};
-  const int rc = lp_solve(p, net, &s);
+  const int rc = lp_solve(p, method == 0 ? net : nullptr, method, &s);
   if (rc < 0) return -1;
   k_lp_expand<<<lp_blocks(nodes), 256>>>(p->S.x, p->pot, p->R, p->np, p->nt);
   if (!cuda_ok(cudaMemcpy(potential_v, p->pot, bytes, cudaMemcpyDeviceToHost), "cudaMemcpy"))
@@ -1077,6 +1250,62 @@ int gcs_mi_solve_conductance_tensor_learned(gcs_mi_net *net,
   }
   if (stats) *stats = s;
   return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// One application, on host vectors of the reduced system (1 + R np
+// doubles), of the scaled operator (what = 1: y = S^-1 A v) or of the
+// preconditioner of `method` (what = 0: y = M v), for the configuration and
+// conductances given -- the pieces of the learned solve, for checking them
+// against a CPU restatement.
+int gcs_mi_learned_apply(gcs_mi_net *net, int method, int what,
+                         const gamera_mi_solver_config *config, const double *pedersen,
+                         const double *hall, const double *v, double *y) {
+  if (!config || !pedersen || !hall || !v || !y || method < 0 || method > 2 || what < 0 ||
+      what > 2 || (method == 0 && !net && what == 2)) {
+    set_api_error("invalid learned MI apply arguments");
+    return -1;
+  }
+  std::lock_guard<std::mutex> lock(g_lp_mutex);
+  gcs_mi_learned_plan *p = lp_create(config, net);
+  if (!p) return -1;
+  const size_t nodes = (size_t)config->longitude_count * config->colatitude_count;
+  std::vector<double> zeros(nodes, 0.0);
+  int rc = -1;
+  const size_t nb = p->n * sizeof(double);
+  if (cuda_ok(cudaMemcpy(p->sp, pedersen, nodes * sizeof(double), cudaMemcpyHostToDevice),
+              "cudaMemcpy") &&
+      cuda_ok(cudaMemcpy(p->sh, hall, nodes * sizeof(double), cudaMemcpyHostToDevice),
+              "cudaMemcpy") &&
+      cuda_ok(cudaMemcpy(p->fac, zeros.data(), nodes * sizeof(double), cudaMemcpyHostToDevice),
+              "cudaMemcpy") &&
+      cuda_ok(cudaMemcpy(p->pot, zeros.data(), nodes * sizeof(double), cudaMemcpyHostToDevice),
+              "cudaMemcpy")) {
+    LpSys &S = p->S;
+    const int H0 = round_up(p->R, 8), W0 = round_up(p->np, 32);
+    k_lp_setup<<<lp_blocks((size_t)p->R * p->np), 256>>>(S);
+    k_lp_dg0<<<1, 32>>>(S);
+    k_lp_ring_setup<<<p->R + 1, 256>>>(S);
+    k_lp_ring_factor<<<1, 1>>>(S);
+    if (method == 0 && what == 0)
+      k_lp_features<<<lp_blocks((size_t)H0 * W0), 256>>>(S, p->net_in, H0, W0);
+    double *dv = p->V, *dy = p->Z;
+    if (cuda_ok(cudaMemcpy(dv, v, nb, cudaMemcpyHostToDevice), "cudaMemcpy")) {
+      bool ok = true;
+      if (what == 1)
+        k_lp_apply<<<lp_blocks(p->n), 256>>>(S, dv, dy, nullptr);
+      else if (what == 2)
+        ok = lp_right(p, method == 0 ? net : nullptr, method, dv, dy);
+      else
+        lp_left(p, method, dv, dy);
+      if (ok && cuda_ok(cudaMemcpy(y, dy, nb, cudaMemcpyDeviceToHost), "cudaMemcpy")) rc = 0;
+    }
+  }
+  lp_free(p);
+  return rc;
 }
 
 }  // extern "C"

@@ -6,10 +6,11 @@ with an auroral ridge, Hall = 1.5 Pedersen), a potential, and the FAC that
 the conductance-tensor operator maps that potential to.  Potentials are
 either random smooth fields (their FAC side is obtained by applying the
 operator with the library's bitwise apply), or the solved potential of a
-Region-1/2 FAC pattern.  The network learns the map from the (row-scaled,
-unit-RMS) residual to the (unit-RMS) potential correction, with the
-conductance and geometry as extra input channels; longitude rotations and
-sign flips augment the pool.
+Region-1/2 FAC pattern.  The network is the flexible right preconditioner
+of the learned solve: it learns the map from v = L A e (L the linear
+two-level left preconditioner, at unit RMS) back to the potential e (in the
+same units), with the conductance and geometry as extra input channels;
+longitude rotations and sign flips augment the pool.
 """
 from __future__ import annotations
 
@@ -52,6 +53,81 @@ def smooth_potential(rng, nt, npl, max_colatitude):
     return e * 1e3
 
 
+def scaled_operator(config, pedersen, hall):
+    """The reduced conductance-tensor system with its rows scaled as in the
+    learned solve (interior rows by sin(theta), the pole by ps / sqrt(np)):
+    returns (A' as a scipy CSR matrix, ring prolongation E).  Stencil as
+    nonorthogonal_mi.c:776-900."""
+    import scipy.sparse as sp
+    nt, npl = config.colatitude_count, config.longitude_count
+    R, n = nt - 2, 1 + (nt - 2) * npl
+    dth = config.maximum_colatitude / (nt - 1)
+    dph = 2.0 * math.pi / npl
+    th = dth * np.arange(nt)
+
+    def inc2(a):
+        c = np.cos(a)
+        return 4.0 * c * c / (1.0 + 3.0 * c * c)
+
+    cinc = config.hemisphere * 2.0 * np.cos(th) / np.sqrt(1.0 + 3.0 * np.cos(th) ** 2)
+    P, H = pedersen, hall
+    i = np.arange(1, nt - 1)[:, None]
+    j = np.arange(npl)[None, :]
+    jm, jp = (j - 1) % npl, (j + 1) % npl
+    ti = th[i]
+    lower = np.sin(ti - dth / 2) * 0.5 * (P[i, j] + P[i - 1, j]) / (inc2(ti - dth / 2) * dth * dth)
+    upper = np.sin(ti + dth / 2) * 0.5 * (P[i, j] + P[i + 1, j]) / (inc2(ti + dth / 2) * dth * dth)
+    llo = 0.5 * (P[i, j] + P[i, jm]) / (np.sin(ti) * dph * dph)
+    lup = 0.5 * (P[i, j] + P[i, jp]) / (np.sin(ti) * dph * dph)
+    f12 = -H / cinc[:, None]
+    dft = (f12[i + 1, j] - f12[i - 1, j]) / (2.0 * dth)
+    dfp = (f12[i, jp] - f12[i, jm]) / (2.0 * dph)
+    s = np.sin(ti)
+    q = 1 + (i - 1) * npl + j
+    below = np.where(i == 1, 0, q - npl)
+    entries = [(q, (lower + upper + llo + lup) / s), (below, (-lower - dfp / (2 * dth)) / s),
+               (1 + (i - 1) * npl + jm, (-llo + dft / (2 * dph)) / s),
+               (1 + (i - 1) * npl + jp, (-lup - dft / (2 * dph)) / s)]
+    rows, cols, vals = [], [], []
+    for c, v in entries:
+        rows.append(np.broadcast_to(q, v.shape).ravel())
+        cols.append(np.broadcast_to(c, v.shape).ravel())
+        vals.append(v.ravel())
+    upm = (i + 2 < nt) & np.ones_like(q, dtype=bool)
+    rows.append(q[upm])
+    cols.append((q + npl)[upm])
+    vals.append(((-upper + dfp / (2 * dth)) / s)[upm])
+    ppm = P[0].mean()
+    pe = np.sin(0.5 * dth) * 0.5 * (ppm + P[1]) / (inc2(0.5 * dth) * dth * dth)
+    ps = npl * (np.sin(0.5 * dth) * config.pedersen_siemens / (inc2(0.5 * dth) * dth * dth))
+    s0 = ps / math.sqrt(npl)
+    rows += [np.array([0]), np.zeros(npl, dtype=np.int64)]
+    cols += [np.array([0]), 1 + np.arange(npl)]
+    vals += [np.array([pe.sum() / s0]), -pe / s0]
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n, n))
+    E = sp.csr_matrix((np.ones(n), (np.arange(n),
+                                    np.concatenate([[0], 1 + np.repeat(np.arange(R), npl)]))),
+                      shape=(n, R + 1))
+    return A, E
+
+
+def two_level(A, E, T, v, omega=0.7):
+    """The learned solve's linear left preconditioner L v: a coarse
+    correction on ring means, two damped Jacobi steps, the coarse correction
+    again (as lp_left in gcs_learn.cu)."""
+    D = A.diagonal()
+    z = E @ T.solve(E.T @ v)
+    for _ in range(2):
+        z = z + omega * (v - A @ z) / D
+    return z + E @ T.solve(E.T @ (v - A @ z))
+
+
+def reduce(field):
+    """Natural nt x np field -> reduced vector (pole, interior rows)."""
+    return np.concatenate([[field[0, 0]], field[1:-1].ravel()])
+
+
 def features(config, pedersen, hall):
     nt = config.colatitude_count
     theta = np.linspace(0.0, config.maximum_colatitude, nt)
@@ -61,7 +137,7 @@ def features(config, pedersen, hall):
 
 
 class Pool:
-    """Training samples: inputs [4][R][np] (residual channel unit RMS) and
+    """Training samples: inputs [4][R][np] (first channel unit RMS) and
     targets [R][np] (unit RMS)."""
 
     def __init__(self, lib, npl=361, nt=181, max_colatitude_deg=45.0, random_fields=384,
@@ -72,15 +148,15 @@ class Pool:
         cond = [cases.mi_case(npl, nt, seed=seed + 17 * c,
                               max_colatitude_deg=max_colatitude_deg) for c in range(conductances)]
         self.triples = 0
+        ops = {}
         for k in range(random_fields):
             case = cond[k % len(cond)]
             cfg = case.config
+            if k % len(cond) not in ops:
+                ops[k % len(cond)] = self._operator(case)
             e = smooth_potential(rng, nt, npl, cfg.maximum_colatitude)
-            ap = np.zeros_like(e)
-            if lib.gamera_mi_apply_conductance_tensor(C.byref(cfg), _ptr(case.pedersen),
-                                                      _ptr(case.hall), _ptr(e), _ptr(ap)) != 0:
-                raise RuntimeError(lib.gcs_last_error().decode())
-            self._add(inputs, targets, ap[1:nt - 1], e[1:nt - 1],
+            A, E, T = ops[k % len(cond)]
+            self._add(inputs, targets, A, E, T, A @ reduce(e), reduce(e),
                       features(cfg, case.pedersen, case.hall))
         for k in range(solved):
             case = cases.mi_case(npl, nt, seed=seed + 1000 + k,
@@ -91,20 +167,34 @@ class Pool:
                                                       _ptr(case.pedersen), _ptr(case.hall),
                                                       _ptr(pot), C.byref(st)) != 0:
                 raise RuntimeError(lib.gcs_last_error().decode())
-            th = np.linspace(0.0, case.config.maximum_colatitude, nt)[1:nt - 1]
-            c = np.cos(th)
-            inc = case.config.hemisphere * 2.0 * c / np.sqrt(1.0 + 3.0 * c * c)
-            u = -(case.config.ionosphere_radius_m ** 2) * case.fac[1:nt - 1] * inc[:, None]
-            self._add(inputs, targets, u, pot[1:nt - 1],
+            A, E, T = self._operator(case)
+            e = reduce(pot)
+            self._add(inputs, targets, A, E, T, A @ e, e,
                       features(case.config, case.pedersen, case.hall))
         self.inputs = np.stack(inputs)
         self.targets = np.stack(targets)
 
-    def _add(self, inputs, targets, r, e, feat):
-        r = r / max(np.sqrt(np.mean(r * r)), 1e-300)
-        e = e / max(np.sqrt(np.mean(e * e)), 1e-300)
-        inputs.append(np.concatenate([r[None].astype(np.float32), feat]))
-        targets.append(e.astype(np.float32))
+    @staticmethod
+    def _operator(case):
+        import scipy.sparse.linalg as spl
+        A, E = scaled_operator(case.config, case.pedersen, case.hall)
+        T = spl.splu((E.T @ A @ E).tocsc())
+        return A, E, T
+
+    def _add(self, inputs, targets, A, E, T, r, e, feat):
+        """The pair the network sees as the right preconditioner of the
+        learned solve: v = L r (L the two-level left preconditioner) at unit
+        RMS, and the error e with L A e = v at unit RMS (a right
+        preconditioner's output scale does not matter to flexible GMRES, and
+        unit-RMS targets keep the training stable)."""
+        v = two_level(A, E, T, r)
+        sv = 1.0 / max(np.sqrt(np.mean(v * v)), 1e-300)
+        se = 1.0 / max(np.sqrt(np.mean(e * e)), 1e-300)
+        R, npl = self.nt - 2, self.npl
+        vi = (sv * v[1:]).reshape(R, npl)
+        ei = (se * e[1:]).reshape(R, npl)
+        inputs.append(np.concatenate([vi[None].astype(np.float32), feat]))
+        targets.append(ei.astype(np.float32))
         self.triples += 1
 
     def batch(self, rng, B, H0, W0):
@@ -158,14 +248,14 @@ def create_net(lib, config, batch=8, seed=3):
     return net
 
 
-def solve(lib, net, case, guess=None):
-    """Learned (net) or Jacobi (net None) FGMRES solve of a case; returns
-    (rc, potential, stats, fallback, seconds)."""
+def solve(lib, net, case, method=0, guess=None):
+    """Learned-solve call for a case (method 0 two-level + network, 1 Jacobi,
+    2 two-level); returns (rc, potential, stats, fallback, seconds)."""
     pot = (case.potential if guess is None else guess).copy()
     st = abi.MiSolverStats()
     fb = C.c_int()
     t = time.perf_counter()
     rc = lib.gcs_mi_solve_conductance_tensor_learned(
-        net, C.byref(case.config), _ptr(case.fac), _ptr(case.pedersen), _ptr(case.hall),
+        net, method, C.byref(case.config), _ptr(case.fac), _ptr(case.pedersen), _ptr(case.hall),
         _ptr(pot), C.byref(st), C.byref(fb))
     return rc, pot, st, fb.value, time.perf_counter() - t

@@ -448,18 +448,31 @@ int gcs_mi_net_train_step(gcs_mi_net *net, const float *inputs, const float *tar
                           int batch, float learning_rate, int update, float *loss);
 /* The conductance-tensor solve (arguments, validation and result as
  * gamera_mi_solve_conductance_tensor, nonorthogonal_mi.h:96-102) by flexible
- * GMRES(40) on the reduced system with its rows scaled so that the residual
- * 2-norm is the reference's residual norm, preconditioned by the network
- * (net, built for interior_rows = colatitude_count - 2 and longitudes =
- * longitude_count) or by Jacobi (net = NULL).  Convergence is judged on the
- * FP64 true residual against the reference's target.  If maximum_iterations
- * pass without convergence, the reference algorithm continues from the
- * iterate and *fallback is set to 1.  No reference counterpart. */
-int gcs_mi_solve_conductance_tensor_learned(gcs_mi_net *net,
+ * GMRES(40) on the reduced system, its rows scaled so that the residual
+ * 2-norm is the reference's residual norm, left-preconditioned by a linear
+ * L and right-preconditioned by a flexible N.  Method 0: L the two-level
+ * step (a coarse correction on ring means -- one value per colatitude ring
+ * and the pole -- two damped Jacobi steps, the coarse correction again) and
+ * N the network (net, built for interior_rows = colatitude_count - 2 and
+ * longitudes = longitude_count); 1: L Jacobi, N the identity; 2: L the
+ * two-level step, N the identity.  Convergence is judged on the FP64 true
+ * residual against the reference's target at every restart.  If
+ * maximum_iterations pass without convergence, the reference algorithm
+ * continues from the iterate and *fallback is set to 1.  No reference
+ * counterpart. */
+int gcs_mi_solve_conductance_tensor_learned(gcs_mi_net *net, int method,
                                             const gamera_mi_solver_config *config,
                                             const double *fac_a_m2, const double *pedersen,
                                             const double *hall, double *potential_v,
                                             gamera_mi_solver_stats *stats, int *fallback);
+/* One application of the learned solve's scaled operator (what = 1), its
+ * left preconditioner L (what = 0) or its right preconditioner N (what = 2)
+ * for `method` to a host vector of the reduced
+ * system (1 + (colatitude_count - 2) longitude_count doubles), for checking
+ * them against a CPU restatement.  No reference counterpart. */
+int gcs_mi_learned_apply(gcs_mi_net *net, int method, int what,
+                         const gamera_mi_solver_config *config, const double *pedersen,
+                         const double *hall, const double *v, double *y);
 
 #ifdef __cplusplus
 }

@@ -147,6 +147,7 @@ def _load(path=None):
     sig["gamera_cs_edge_sync_plan_destroy"] = (None, [C.c_void_p])
     sig["gamera_cs_sync_edge_emf_planned"] = (C.c_int, [C.c_void_p, P(abi.Storage)])
     sig.update(abi.mi_dipole_signatures())
+    sig.update(abi.ensemble_signatures())
     sig["gcs_context_mi_dipole_create"] = (
         C.c_int, [C.c_void_p, P(abi.EarthStartup), P(abi.MiDipoleConfig),
                   P(C.c_void_p)])

@@ -218,6 +218,48 @@ class MiAnalysisView(C.Structure):
                 ("potential_v", C.POINTER(C.c_double) * 2)]
 
 
+class WindDriver(C.Structure):
+    """gcs_wind_driver: upstream n (cm^-3), Vx (km/s), T (K), IMF Bz (nT)."""
+    _fields_ = [("density_cm3", C.c_double), ("velocity_x_kms", C.c_double),
+                ("temperature_k", C.c_double), ("bz_nt", C.c_double)]
+
+
+class EnsembleConfig(C.Structure):
+    """gcs_ensemble_config."""
+    _fields_ = [("count", C.c_int), ("nr", C.POINTER(C.c_size_t)),
+                ("n", C.POINTER(C.c_size_t)), ("drivers", C.POINTER(WindDriver)),
+                ("seed", C.c_ulonglong), ("fp32_bulk", C.c_int),
+                ("autotune_repetitions", C.c_int), ("dt_fraction", C.c_double)]
+
+
+def ensemble_signatures():
+    P = C.POINTER
+    return {
+        "gcs_context_create_wind": (C.c_void_p, [C.c_size_t, C.c_size_t, C.c_ulonglong,
+                                                 P(WindDriver)]),
+        "gcs_tile_limit": (C.c_int, [C.c_int]),
+        "gcs_context_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+        "gcs_context_tile": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int), P(C.c_int)]),
+        "gcs_context_autotune": (C.c_int, [C.c_void_p, P(AdvanceOptions),
+                                           P(TimestepOptions), C.c_int, P(C.c_double),
+                                           P(C.c_double)]),
+        "gcs_ensemble_draw": (C.c_int, [C.c_ulonglong, C.c_int, P(C.c_size_t),
+                                        P(WindDriver)]),
+        "gcs_ensemble_estimate_bytes": (C.c_double, [C.c_int, P(C.c_size_t),
+                                                     P(C.c_size_t), C.c_int]),
+        "gcs_ensemble_create": (C.c_void_p, [P(EnsembleConfig)]),
+        "gcs_ensemble_destroy": (None, [C.c_void_p]),
+        "gcs_ensemble_count": (C.c_int, [C.c_void_p]),
+        "gcs_ensemble_run_context": (C.c_void_p, [C.c_void_p, C.c_int]),
+        "gcs_ensemble_grid_owner": (C.c_int, [C.c_void_p, C.c_int]),
+        "gcs_ensemble_advance": (C.c_int, [C.c_void_p, C.c_int]),
+        "gcs_ensemble_sync": (C.c_int, [C.c_void_p, P(C.c_int)]),
+        "gcs_ensemble_stream": (C.c_size_t, [C.c_void_p]),
+        "gcs_ensemble_device_bytes": (C.c_size_t, [C.c_void_p]),
+        "gcs_ensemble_graph_info": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int)]),
+    }
+
+
 def mi_dipole_signatures():
     """ctypes signatures of the cubedsphere_mi_dipole.h entry points, shared
     by this library and the reference build."""

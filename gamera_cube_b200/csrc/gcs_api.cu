@@ -14,12 +14,6 @@
 #include <new>
 #include <vector>
 
-struct gcs_context {
-  gcs::Context c;
-  std::vector<cudaEvent_t> events;   // profiling: 2 per recorded stage
-  std::vector<int> event_slot;
-};
-
 struct gamera_cs_halo_plan {
   gcs_context *ctx;
 };
@@ -546,6 +540,16 @@ Context *context_for_grid(const gamera_no_grid grid[6], const size_t active[3],
   return ctx ? &ctx->c : nullptr;
 }
 Context *context_of(gcs_context *ctx) { return ctx ? &ctx->c : nullptr; }
+bool driver_opts(const gamera_no_advance_options *options,
+                 const gamera_no_timestep_options *t, double fraction, Opts *O) {
+  if (!std::isfinite(fraction) || fraction <= 0.0) return false;
+  if (!make_opts(options, true, O) || !set_timestep_opts(t, O)) return false;
+  O->dt_fraction = fraction;
+  return true;
+}
+int enqueue_driver_step(gcs_context *ctx, const Opts &O) {
+  return run_step(ctx, O, 1, nullptr);
+}
 }  // namespace gcs
 
 extern "C" {
@@ -992,6 +996,9 @@ int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
     const unsigned char *b = (const unsigned char *)&O;
     for (size_t q = 0; q < sizeof(O); ++q) key = (key ^ b[q]) * 1099511628211ULL;
     key = (key ^ (unsigned long long)C.X.bulk) * 1099511628211ULL;
+    for (int f = 0; f < gcs::kTileFamilies; ++f)
+      key = (key ^ (unsigned long long)(C.X.tile[f].bx * 64 + C.X.tile[f].by)) *
+            1099511628211ULL;
     if (!C.graph_exec || C.graph_key != key) {
       if (C.graph_exec) cudaGraphExecDestroy(C.graph_exec);
       C.graph_exec = nullptr;

@@ -538,8 +538,8 @@ __device__ inline uint64_t splitmix(uint64_t x) {
 // uniform MHD state, radial shock, solar wind with seeded noise, wind with
 // a density pulse).
 __global__ void k_init_cells(Dims D, int f, int kind, unsigned long long seed,
-                             const gamera_no_cell_geometry *cells, DevState S,
-                             int *bad) {
+                             WindInit w, const gamera_no_cell_geometry *cells,
+                             DevState S, int *bad) {
   const long long t = tid();
   if (t >= (long long)D.E0 * D.E1 * D.E2) return;
   const int i = (int)(t / ((long long)D.E1 * D.E2));
@@ -558,10 +558,9 @@ __global__ void k_init_cells(Dims D, int f, int kind, unsigned long long seed,
     const uint64_t h = splitmix(splitmix((uint64_t)seed) ^ ((uint64_t)f << 56) ^
                                 (uint64_t)t);
     const double noise = 2.0 * ((double)(h >> 11) * 0x1.0p-53) - 1.0;
-    double rho = 5.0 * (1.0 + 0.01 * noise);
-    if (kind == 3) rho *= 1.0 + 0.2 * sin(2.0 * acos(-1.0) * x.value[0] / 10.0);
-    const double pres = 5.0e6 * 1.380649e-23 * 1.0e5 / (1.67262192369e-21 * 1.0e10);
-    p = {rho, kind == 3 ? -4.5 : -4.0, 0.0, 0.0, pres};
+    double rho = w.rho * (1.0 + 0.01 * noise);
+    if (w.pulse) rho *= 1.0 + 0.2 * sin(2.0 * acos(-1.0) * x.value[0] / 10.0);
+    p = {rho, w.vx, 0.0, 0.0, w.pres};
     rf = 1e-6;
     pf = 1e-8;
   }
@@ -672,11 +671,37 @@ __global__ void k_init_b(Dims D, DevState S, DevGeom G, int *bad) {
     }                                                  \
   } while (0)
 
-int Context::init_case(int kind, size_t nr, size_t n, unsigned long long seed) {
-  if (kind < 0 || kind > 3) {
+WindInit case_wind(int kind) {
+  const double bnorm = 100000.0 * sqrt(4.0e-7 * acos(-1.0) * 1.67262192369e-21);
+  WindInit w;
+  w.rho = 5.0;
+  w.vx = kind == 3 ? -4.5 : -4.0;
+  w.pres = 5.0e6 * 1.380649e-23 * 1.0e5 / (1.67262192369e-21 * 1.0e10);
+  w.bz = -5.0e-9 / bnorm;
+  w.pulse = kind == 3;
+  return w;
+}
+
+WindInit driven_wind(double density_cm3, double velocity_x_kms, double temperature_k,
+                     double bz_nt) {
+  const double bnorm = 100000.0 * sqrt(4.0e-7 * acos(-1.0) * 1.67262192369e-21);
+  WindInit w;
+  w.rho = density_cm3;
+  w.vx = velocity_x_kms / 100.0;
+  w.pres = density_cm3 * 1.0e6 * 1.380649e-23 * temperature_k /
+           (1.67262192369e-21 * 1.0e10);
+  w.bz = bz_nt * 1.0e-9 / bnorm;
+  w.pulse = 0;
+  return w;
+}
+
+int Context::init_case(int kind, size_t nr, size_t n, unsigned long long seed,
+                       const WindInit *driver) {
+  if (kind < 0 || kind > 3 || (driver && kind != 2)) {
     set_error("unknown case kind", "init_case");
     return -1;
   }
+  const WindInit wi = driver ? *driver : case_wind(kind);
   const int wind = kind >= 2;
   const size_t active[3] = {nr, n, n};
   if (allocate(active, 4) != 0) return -1;
@@ -700,8 +725,7 @@ int Context::init_case(int kind, size_t nr, size_t n, unsigned long long seed) {
   GCS_BTRY(cudaMalloc(&d_cen, fmax * sizeof(gamera_no_vec3)));
   GCS_BTRY(cudaMalloc(&d_av, 3 * fmax * sizeof(gamera_no_vec3)));
   const V3 m = {0.0, 0.0, -6761.730688424097};
-  const double bnorm = 100000.0 * sqrt(4.0e-7 * acos(-1.0) * 1.67262192369e-21);
-  const V3 bimf = {0.0, 0.0, -5.0e-9 / bnorm};
+  const V3 bimf = {0.0, 0.0, wi.bz};
   const V3 bu = kind == 0 ? V3{0.38, -0.21, 0.16} : V3{0.1, 0.08, -0.03};
   const int bs = 128;
   for (int f = 0; f < kFaces; ++f) {
@@ -745,8 +769,8 @@ int Context::init_case(int kind, size_t nr, size_t n, unsigned long long seed) {
                            (D.E2 + (d != 2));
       k_edges<<<nblk(ec, bs), bs, 0, stream>>>(D, f, d, vert, X.G, bad);
     }
-    k_init_cells<<<nblk(cells, bs), bs, 0, stream>>>(D, f, kind, seed, acells, X.S,
-                                                     bad);
+    k_init_cells<<<nblk(cells, bs), bs, 0, stream>>>(D, f, kind, seed, wi, acells,
+                                                     X.S, bad);
     if (wind) {
       if (!bg_pool && allocate_background() != 0) return -1;
       for (int d = 0; d < 3; ++d) {
@@ -795,6 +819,93 @@ int Context::init_case(int kind, size_t nr, size_t n, unsigned long long seed) {
     }
   }
   return build_plans(geo);
+}
+
+// A wind run on the grid of `o` (same extents, built by init_case): the
+// geometry, background, halo/seam/edge plans, FP32 metric copies and the
+// per-step scratch arrays are o's; this context owns only the state that
+// lives from step to step (U, Uo, B, Bo, Phi, Phi_old), its step
+// parameters, status and stream.  Runs sharing a grid must not step
+// concurrently (they share the scratch arrays).
+int Context::init_member(Context &o, unsigned long long seed, const WindInit &w) {
+  if (!o.bg_uploaded || !o.pool || o.owner) {
+    set_error("owner is not a device-built wind case", "init_member");
+    return -1;
+  }
+  X = o.X;
+  X.params = nullptr;
+  X.status = nullptr;
+  owner = &o;
+  bg_uploaded = 1;
+  bulk_b0_threshold = o.bulk_b0_threshold;
+  const Dims &D = X.D;
+  GCS_BTRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  const long long per = kFaces * D.Nn;
+  pool_bytes = (size_t)22 * per * sizeof(double);
+  GCS_BTRY(cudaMalloc(&pool, pool_bytes));
+  GCS_BTRY(cudaMemsetAsync(pool, 0, pool_bytes, stream));
+  double *p = (double *)pool;
+  DevState &S = X.S;
+  for (int m = 0; m < 5; ++m) {
+    S.U[m] = p; p += per;
+    S.Uo[m] = p; p += per;
+  }
+  for (int m = 0; m < 3; ++m) {
+    S.B[m] = p; p += per;
+    S.Bo[m] = p; p += per;
+    S.P[m] = p; p += per;
+    S.Po[m] = p; p += per;
+  }
+  GCS_BTRY(cudaMalloc(&X.params, sizeof(StepParams)));
+  GCS_BTRY(cudaMalloc(&X.status, sizeof(DevStatus)));
+  GCS_BTRY(cudaMemsetAsync(X.params, 0, sizeof(StepParams), stream));
+  reset_status_async();
+  // The initial state as init_case builds it for a wind case: vertices and
+  // cell centroids of each face rebuilt into scratch (o's staging buffer
+  // holds the cell geometry), the IMF edge integrals, Phi and the recovered
+  // cell B on the shared recovery maps.
+  const long long cells = (long long)D.E0 * D.E1 * D.E2;
+  const long long verts = (long long)(D.E0 + 1) * (D.E1 + 1) * (D.E2 + 1);
+  void *work = nullptr;
+  const size_t wbytes = verts * sizeof(V3) + 3 * D.Nn * sizeof(double) + sizeof(int);
+  GCS_BTRY(cudaMalloc(&work, wbytes));
+  V3 *vert = (V3 *)work;
+  double *line = (double *)(vert + verts);
+  int *bad = (int *)(line + 3 * D.Nn);
+  GCS_BTRY(cudaMemsetAsync(bad, 0, sizeof(int), stream));
+  gamera_no_cell_geometry *acells = (gamera_no_cell_geometry *)o.staging;
+  const V3 bimf = {0.0, 0.0, w.bz};
+  const int bs = 128;
+  for (int f = 0; f < kFaces; ++f) {
+    k_vertices<<<nblk(verts, bs), bs, 0, stream>>>(f, D.nr, D.n, D.g, 2.5, 30.0,
+                                                   log(12.0), vert);
+    k_cells<<<nblk(cells, 64), 64, 0, stream>>>(D, vert, acells, bad);
+    k_init_cells<<<nblk(cells, bs), bs, 0, stream>>>(D, f, 2, seed, w, acells, X.S,
+                                                     bad);
+    for (int e = 0; e < 3; ++e) {
+      const long long ec = (long long)(D.E0 + (e != 0)) * (D.E1 + (e != 1)) *
+                           (D.E2 + (e != 2));
+      k_init_lines<<<nblk(ec, bs), bs, 0, stream>>>(D, e, vert, bimf, line);
+    }
+    for (int d = 0; d < 3; ++d) {
+      const long long fc = (long long)(D.E0 + (d == 0)) * (D.E1 + (d == 1)) *
+                           (D.E2 + (d == 2));
+      k_init_flux<<<nblk(fc, bs), bs, 0, stream>>>(D, f, d, line, 0, V3{0.0, 0.0, 0.0},
+                                                   nullptr, X.S);
+    }
+    GCS_BTRY(cudaGetLastError());
+    GCS_BTRY(cudaStreamSynchronize(stream));
+  }
+  k_init_b<<<nblk(kFaces * cells, bs), bs, 0, stream>>>(D, X.S, X.G, bad);
+  int hbad = 0;
+  GCS_BTRY(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  GCS_BTRY(cudaStreamSynchronize(stream));
+  cudaFree(work);
+  if (hbad) {
+    set_error("degenerate geometry or invalid initial state", "init_member");
+    return -1;
+  }
+  return 0;
 }
 
 }  // namespace gcs

@@ -18,6 +18,12 @@ enum ArrayKind {
   kArrP, kArrPo, kArrPp, kArrF, kArrM, kArrE
 };
 
+// Wind states of the case kinds 2 and 3, and of an explicit upstream
+// driver (n in cm^-3, Vx in km/s, T in K, Bz in nT) (gcs_build.cu).
+WindInit case_wind(int kind);
+WindInit driven_wind(double density_cm3, double velocity_x_kms, double temperature_k,
+                     double bz_nt);
+
 struct Context {
   Ctx X;
   cudaStream_t stream = nullptr;
@@ -57,7 +63,13 @@ struct Context {
            size_t ghost);
   // Build a case (kind, sizes, seed) directly on the device
   // (gcs_build.cu); no host grid is involved.
-  int init_case(int kind, size_t nr, size_t n, unsigned long long seed);
+  int init_case(int kind, size_t nr, size_t n, unsigned long long seed,
+                const WindInit *driver = nullptr);
+  // A wind run on the grid of `o` with its own state (gcs_build.cu).
+  int init_member(Context &o, unsigned long long seed, const WindInit &w);
+  // Non-null for a run sharing the grid of another context; only the state
+  // arrays, params, status and stream are this context's.
+  Context *owner = nullptr;
   int allocate(const size_t active[3], size_t ghost);
   int init_topology(const size_t active[3], size_t ghost);
   int allocate_background();
@@ -91,3 +103,10 @@ struct Context {
 };
 
 }  // namespace gcs
+
+// The C handle of a context (gamera_cs_b200.h).
+struct gcs_context {
+  gcs::Context c;
+  std::vector<cudaEvent_t> events;   // profiling: 2 per recorded stage
+  std::vector<int> event_slot;
+};

@@ -92,6 +92,14 @@ struct Bulk {
   const T *fb0[3][3], *fb0n[3], *eb0t1[3], *eb0t2[3];
 };
 
+// Upstream solar-wind state of a wind case in code units: density (proton
+// cm^-3, before the seeded +-1% noise), Vx (100 km/s), pressure, IMF Bz and
+// the density-pulse flag.
+struct WindInit {
+  double rho, vx, pres, bz;
+  int pulse;
+};
+
 // Scalar parameters of one step.  dt and ratio live in device memory so a
 // captured CUDA graph can advance its own time step.
 struct StepParams {

@@ -20,17 +20,21 @@ __device__ inline bool failed(const DevStatus *st) {
   return *(volatile const unsigned long long *)&st->first != 0ULL;
 }
 
-// Box iteration: grid.x over j*k of the box, grid.y over i, grid.z face.
+// Box iteration over radial layers [i0, i1): a thread block is a tile of
+// blockDim.x consecutive points of the flattened (j, k) plane times
+// blockDim.y consecutive layers; grid.x over j*k, grid.y over the layer
+// groups, grid.z face.
 struct Box {
-  int i0, j0, k0, nj, nk;
+  int i0, j0, k0, nj, nk, i1;
 };
 
 __device__ inline bool box_coord(const Box &b, int *f, int *i, int *j,
                                  int *k) {
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
-  if (jk >= b.nj * b.nk) return false;
+  const int ii = b.i0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (jk >= b.nj * b.nk || ii >= b.i1) return false;
   *f = blockIdx.z;
-  *i = b.i0 + blockIdx.y;
+  *i = ii;
   *j = b.j0 + jk / b.nk;
   *k = b.k0 + jk % b.nk;
   return true;

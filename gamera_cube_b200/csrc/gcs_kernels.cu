@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(256) k_recover(Dims D, DevState S, DevGeom G,
   const bool skip = failed(st);
   const int with_cfl = mode & 2;
   int f, i, j, k;
-  const Box b{0, 0, 0, D.E1, D.E2};
+  const Box b{0, 0, 0, D.E1, D.E2, D.E0};
   double cand = DBL_MAX;
   if (!skip && box_coord(b, &f, &i, &j, &k)) {
     const long long c = f * D.Nn + D.node(i, j, k);
@@ -304,11 +304,12 @@ __global__ void __launch_bounds__(256) k_recover(Dims D, DevState S, DevGeom G,
   for (int o = 16; o > 0; o >>= 1)
     cand = fmin(cand, __shfl_down_sync(0xffffffffu, cand, o));
   __shared__ double wmin[8];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lt = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = lt & 31, warp = lt >> 5;
   if (lane == 0) wmin[warp] = cand;
   __syncthreads();
   if (warp == 0) {
-    cand = lane < (int)(blockDim.x >> 5) ? wmin[lane] : DBL_MAX;
+    cand = lane < (int)((blockDim.x * blockDim.y) >> 5) ? wmin[lane] : DBL_MAX;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
       cand = fmin(cand, __shfl_down_sync(0xffffffffu, cand, o));
@@ -337,10 +338,6 @@ __global__ void k_count_step(StepParams *prm) { prm->step += 1; }
 
 // ---------------------------------------------------------------------------
 // Host-side launchers.
-
-static inline dim3 box_grid(int I, int J, int K, int bs) {
-  return dim3((unsigned)((J * K + bs - 1) / bs), (unsigned)I, kFaces);
-}
 
 Bulk<double> bulk64(const Ctx &X) {
   Bulk<double> B{};
@@ -421,7 +418,8 @@ void launch_halo(const Ctx &X, cudaStream_t s) {
 }
 
 void launch_predict(const Ctx &X, const Opts &O, cudaStream_t s) {
-  k_predict<<<box_grid(X.D.E0 + 1, X.D.N1, X.D.N2, 128), 128, 0, s>>>(
+  const Tile t = X.tile[kTilePredict];
+  k_predict<<<tile_grid(X.D.E0 + 1, X.D.N1, X.D.N2, t), tile_block(t), 0, s>>>(
       X.D, X.S, X.G, X.B32, X.bulk, O, X.params, X.status);
 }
 
@@ -435,13 +433,22 @@ void launch_flux(const Ctx &X, const Opts &O, cudaStream_t s) {
   if (X.bulk) launch_flux_f32(X, O, sp, X.D.E0 + 1, s);
 }
 
-void launch_emf(const Ctx &X, const Opts &O, cudaStream_t s) {
+void launch_face_velocities(const Ctx &X, const Opts &O, cudaStream_t s) {
   const int sp = bulk_split(X);
-  // every face velocity before any edge EMF reads them
   Sweeps<double>::emf(X, bulk64(X), O, 0, sp, s);
   if (X.bulk) launch_face_velocity_f32(X, O, sp, X.D.E0 + 1, s);
+}
+
+void launch_edge_emfs(const Ctx &X, const Opts &O, cudaStream_t s) {
+  const int sp = bulk_split(X);
   Sweeps<double>::edge(X, bulk64(X), O, 0, sp, s);
   if (X.bulk) launch_edge_emf_f32(X, O, sp, X.D.E0 + 1, s);
+}
+
+void launch_emf(const Ctx &X, const Opts &O, cudaStream_t s) {
+  // every face velocity before any edge EMF reads them
+  launch_face_velocities(X, O, s);
+  launch_edge_emfs(X, O, s);
 }
 
 void launch_edge_sync(const Ctx &X, cudaStream_t s) {
@@ -452,26 +459,29 @@ void launch_edge_sync(const Ctx &X, cudaStream_t s) {
 
 void launch_update(const Ctx &X, const Opts &O, cudaStream_t s) {
   const Dims &D = X.D;
-  k_ct<0><<<box_grid(D.E0 + 1, D.E1, D.E2, 128), 128, 0, s>>>(D, X.S, O, X.params,
-                                                              X.status);
-  k_ct<1><<<box_grid(D.E0, D.E1 + 1, D.E2, 128), 128, 0, s>>>(D, X.S, O, X.params,
-                                                              X.status);
-  k_ct<2><<<box_grid(D.E0, D.E1, D.E2 + 1, 128), 128, 0, s>>>(D, X.S, O, X.params,
-                                                              X.status);
-  k_update<<<box_grid(D.E0, D.E1, D.E2, 128), 128, 0, s>>>(D, X.S, X.G, X.BG, O,
-                                                           X.params, X.status);
+  const Tile t = X.tile[kTileCt], tu = X.tile[kTileUpdate];
+  k_ct<0><<<tile_grid(D.E0 + 1, D.E1, D.E2, t), tile_block(t), 0, s>>>(
+      D, X.S, O, X.params, X.status);
+  k_ct<1><<<tile_grid(D.E0, D.E1 + 1, D.E2, t), tile_block(t), 0, s>>>(
+      D, X.S, O, X.params, X.status);
+  k_ct<2><<<tile_grid(D.E0, D.E1, D.E2 + 1, t), tile_block(t), 0, s>>>(
+      D, X.S, O, X.params, X.status);
+  k_update<<<tile_grid(D.E0, D.E1, D.E2, tu), tile_block(tu), 0, s>>>(
+      D, X.S, X.G, X.BG, O, X.params, X.status);
 }
 
 void launch_recover(const Ctx &X, const Opts &O, int with_cfl,
                     cudaStream_t s) {
   const Dims &D = X.D;
-  k_recover<<<box_grid(D.E0, D.E1, D.E2, 256), 256, 0, s>>>(
+  const Tile t = X.tile[kTileRecover];
+  k_recover<<<tile_grid(D.E0, D.E1, D.E2, t), tile_block(t), 0, s>>>(
       D, X.S, X.G, X.BG, O, 1 | (with_cfl ? 2 : 0), X.status);
 }
 
 void launch_timestep(const Ctx &X, const Opts &O, cudaStream_t s) {
   const Dims &D = X.D;
-  k_recover<<<box_grid(D.E0, D.E1, D.E2, 256), 256, 0, s>>>(
+  const Tile t = X.tile[kTileRecover];
+  k_recover<<<tile_grid(D.E0, D.E1, D.E2, t), tile_block(t), 0, s>>>(
       D, X.S, X.G, X.BG, O, 2, X.status);
 }
 

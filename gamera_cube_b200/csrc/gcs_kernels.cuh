@@ -7,8 +7,23 @@
 
 namespace gcs {
 
+// Launch tile of a kernel family: blockDim.x consecutive points of the
+// flattened (j, k) plane of a radial layer times blockDim.y layers.  The
+// kernels compute per point, so the tile changes speed only, never results.
+enum TileFamily {
+  kTilePredict = 0, kTileFlux, kTileFaceVelocity, kTileEdgeEmf, kTileCt,
+  kTileUpdate, kTileRecover, kTileFamilies
+};
+struct Tile {
+  int bx, by;
+};
+// Largest tile (bx * by) each family's kernels are compiled for.
+constexpr int kTileMaxThreads[kTileFamilies] = {256, 128, 256, 128, 256, 128, 256};
+
 struct Ctx {
   Dims D;
+  Tile tile[kTileFamilies] = {{128, 1}, {128, 1}, {128, 1}, {128, 1},
+                              {128, 1}, {128, 1}, {256, 1}};
   DevState S;
   DevGeom G;
   DevBg BG;
@@ -27,6 +42,13 @@ struct Ctx {
   Bulk<float> B32{};
 };
 
+// Grid of a tile over radial layers [0, I) and a J x K plane, six faces.
+inline dim3 tile_grid(int I, int J, int K, Tile t) {
+  return dim3((unsigned)((J * K + t.bx - 1) / t.bx), (unsigned)((I + t.by - 1) / t.by),
+              kFaces);
+}
+inline dim3 tile_block(Tile t) { return dim3((unsigned)t.bx, (unsigned)t.by, 1); }
+
 // Bulk<double> view of the FP64 arrays.
 Bulk<double> bulk64(const Ctx &X);
 
@@ -44,6 +66,9 @@ void launch_radial_outflow_all(const Ctx &X, cudaStream_t s);
 void launch_predict(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_flux(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_emf(const Ctx &X, const Opts &O, cudaStream_t s);
+// The two halves of launch_emf: face velocities, then edge EMFs.
+void launch_face_velocities(const Ctx &X, const Opts &O, cudaStream_t s);
+void launch_edge_emfs(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_edge_sync(const Ctx &X, cudaStream_t s);
 void launch_update(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_recover(const Ctx &X, const Opts &O, int with_cfl,

@@ -662,6 +662,10 @@ int Context::allocate_background() {
 }
 
 int Context::upload_background(const gamera_no_background_field bg[kFaces]) {
+  if (owner) {
+    set_error("the background of a shared grid belongs to its owner", "upload_background");
+    return -1;
+  }
   const Dims &D = X.D;
   if (!bg_pool && allocate_background() != 0) return -1;
   const size_t cells = (size_t)D.E0 * D.E1 * D.E2;
@@ -756,6 +760,12 @@ int Context::transfer_array(int f, int kind, int dir, bool upload, double *host)
   }
   const long long count = (long long)e[0] * e[1] * e[2];
   const size_t bytes = (size_t)count * ncomp * sizeof(double);
+  if (!staging && owner) {
+    // runs sharing a grid allocate their transfer buffer on first use: the
+    // largest state array of one face (5 doubles per node)
+    staging_bytes = (size_t)(D.E0 + 1) * (D.E1 + 1) * (D.E2 + 1) * 5 * sizeof(double);
+    GCS_TRY(cudaMalloc(&staging, staging_bytes));
+  }
   if (bytes > staging_bytes) {
     set_error("staging too small", "transfer");
     return -1;
@@ -873,6 +883,16 @@ __global__ void k_layer_b0(Dims D, DevBg BG, unsigned long long *layer_max) {
 // normal 3, edge B0 projections 6).  The sweep outputs stay the FP64
 // arrays of the state.
 int Context::enable_bulk(int on) {
+  if (owner) {
+    if (on && !owner->X.bulk) {
+      set_error("switch the grid owner to FP32-bulk first", "enable_bulk");
+      return -1;
+    }
+    X.B32 = owner->X.B32;
+    X.bulk_split = owner->X.bulk_split;
+    X.bulk = on ? 1 : 0;
+    return 0;
+  }
   if (!on) {
     X.bulk = 0;
     return 0;
@@ -969,6 +989,10 @@ int Context::enable_bulk(int on) {
 // Radial layers whose largest cell |B0| exceeds the threshold, and all
 // layers inside them, keep the FP64 sweeps.
 int Context::set_bulk_split(double b0_threshold) {
+  if (owner) {
+    set_error("the FP64 layers of a shared grid are its owner's", "set_bulk_split");
+    return -1;
+  }
   bulk_b0_threshold = b0_threshold;
   const Dims &D = X.D;
   X.bulk_split = 0;

@@ -32,7 +32,7 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
                           Opts O, const StepParams *prm, DevStatus *st) {
   if (failed(st)) return;
   int f, i, j, k;
-  const Box b{0, 0, 0, D.N1, D.N2};
+  const Box b{0, 0, 0, D.N1, D.N2, D.E0 + 1};
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const double r = prm->ratio;
   const long long c = f * D.Nn + D.node(i, j, k);
@@ -107,10 +107,11 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
 // one stencil and the reconstructed face states are live at once.
 template <int d, typename T>
 __global__ void __launch_bounds__(128, 4) k_flux(Dims D, DevState S, Bulk<T> B,
-                                                 Opts O, DevStatus *st, int i0) {
+                                                 Opts O, DevStatus *st, int i0,
+                                                 int i1) {
   if (failed(st)) return;
   int f, i, j, k;
-  const Box b{i0, D.g, D.g, D.n + (d == 1), D.n + (d == 2)};
+  const Box b{i0, D.g, D.g, D.n + (d == 1), D.n + (d == 2), i1};
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const long long c = f * D.Nn + D.node(i, j, k);
   const long long sd = D.stride(d);
@@ -264,7 +265,8 @@ __global__ void k_seam_flux(Dims D, const Seam *seams, DevState S, DevStatus *st
 // central8 of the per-cell weights over central8 of the volumes, for every
 // face the edge velocities of edge family (a+2)%3 read.
 template <int a, typename T>
-__global__ void k_face_velocity(Dims D, Bulk<T> B, DevStatus *st, int i0) {
+__global__ void k_face_velocity(Dims D, Bulk<T> B, DevStatus *st, int i0,
+                                int i1) {
   if (failed(st)) return;
   constexpr int e = (a + 2) % 3, bb = (a + 1) % 3;
   int f, x[3];
@@ -272,7 +274,7 @@ __global__ void k_face_velocity(Dims D, Bulk<T> B, DevStatus *st, int i0) {
   lo[e] = D.g; cnt[e] = D.act(e);
   lo[a] = D.g; cnt[a] = D.act(a) + 1;
   lo[bb] = 0; cnt[bb] = D.ext(bb);
-  const Box b{i0, lo[1], lo[2], cnt[1], cnt[2]};
+  const Box b{i0, lo[1], lo[2], cnt[1], cnt[2], i1};
   if (!box_coord(b, &f, &x[0], &x[1], &x[2])) return;
   const long long c = f * D.Nn + D.node(x[0], x[1], x[2]);
   const long long sa = D.stride(a);
@@ -292,7 +294,8 @@ template <int e, typename T>
 __global__ void __launch_bounds__(128) k_edge_emf(Dims D, DevState S, DevGeom G,
                                                   Bulk<T> B, Opts O,
                                                   const StepParams *prm,
-                                                  DevStatus *st, int i0) {
+                                                  DevStatus *st, int i0,
+                                                  int i1) {
   if (failed(st)) return;
   constexpr int a = (e + 1) % 3, bb = (e + 2) % 3;
   int f, x[3];
@@ -300,7 +303,7 @@ __global__ void __launch_bounds__(128) k_edge_emf(Dims D, DevState S, DevGeom G,
   cnt[e] = D.act(e);
   cnt[a] = D.act(a) + 1;
   cnt[bb] = D.act(bb) + 1;
-  const Box b{i0, D.g, D.g, cnt[1], cnt[2]};
+  const Box b{i0, D.g, D.g, cnt[1], cnt[2], i1};
   if (!box_coord(b, &f, &x[0], &x[1], &x[2])) return;
   const long long c = f * D.Nn + D.node(x[0], x[1], x[2]);
   const unsigned char ok = G.edge_ok[e][c];
@@ -398,7 +401,7 @@ template <int d>
 __global__ void k_ct(Dims D, DevState S, Opts O, const StepParams *prm, DevStatus *st) {
   if (failed(st)) return;
   int f, i, j, k;
-  const Box b{0, 0, 0, D.E1 + (d == 1), D.E2 + (d == 2)};
+  const Box b{0, 0, 0, D.E1 + (d == 1), D.E2 + (d == 2), D.E0 + (d == 0)};
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const long long c = f * D.Nn + D.node(i, j, k);
   const double old = S.P[d][c];
@@ -430,7 +433,7 @@ __global__ void __launch_bounds__(128) k_update(Dims D, DevState S, DevGeom G,
                                                 DevStatus *st) {
   if (failed(st)) return;
   int f, i, j, k;
-  const Box b{0, 0, 0, D.E1, D.E2};
+  const Box b{0, 0, 0, D.E1, D.E2, D.E0};
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const long long c = f * D.Nn + D.node(i, j, k);
   double u[5], bo[3];
@@ -512,10 +515,6 @@ __global__ void __launch_bounds__(128) k_update(Dims D, DevState S, DevGeom G,
 // of the range each sweep covers (clamped to it; empty ranges launch
 // nothing).
 
-inline dim3 sweep_grid(int I, int J, int K, int bs) {
-  return dim3((unsigned)((J * K + bs - 1) / bs), (unsigned)I, kFaces);
-}
-
 inline bool clamp_range(int lo, int hi, int i0, int i1, int *a, int *n) {
   *a = lo > i0 ? lo : i0;
   const int b = hi < i1 ? hi : i1;
@@ -529,43 +528,47 @@ struct Sweeps {
                    cudaStream_t s) {
     const Dims &D = X.D;
     int a, n;
+    const Tile t = X.tile[kTileFlux];
     if (clamp_range(D.g, D.g + D.nr + 1, i0, i1, &a, &n))
-      k_flux<0, T><<<sweep_grid(n, D.n, D.n, 128), 128, 0, s>>>(D, X.S, B, O, X.status, a);
+      k_flux<0, T><<<tile_grid(n, D.n, D.n, t), tile_block(t), 0, s>>>(
+          D, X.S, B, O, X.status, a, a + n);
     if (clamp_range(D.g, D.g + D.nr, i0, i1, &a, &n))
-      k_flux<1, T><<<sweep_grid(n, D.n + 1, D.n, 128), 128, 0, s>>>(D, X.S, B, O,
-                                                                     X.status, a);
+      k_flux<1, T><<<tile_grid(n, D.n + 1, D.n, t), tile_block(t), 0, s>>>(
+          D, X.S, B, O, X.status, a, a + n);
     if (clamp_range(D.g, D.g + D.nr, i0, i1, &a, &n))
-      k_flux<2, T><<<sweep_grid(n, D.n, D.n + 1, 128), 128, 0, s>>>(D, X.S, B, O,
-                                                                     X.status, a);
+      k_flux<2, T><<<tile_grid(n, D.n, D.n + 1, t), tile_block(t), 0, s>>>(
+          D, X.S, B, O, X.status, a, a + n);
   }
   static void emf(const Ctx &X, const Bulk<T> &B, const Opts &O, int i0, int i1,
                   cudaStream_t s) {
     const Dims &D = X.D;
     int a, n;
     // face velocities: family a, edge family e=(a+2)%3 active, a faces, bb all
+    const Tile t = X.tile[kTileFaceVelocity];
     if (clamp_range(D.g, D.g + D.nr + 1, i0, i1, &a, &n))  // e=2, a=0, bb=1
-      k_face_velocity<0, T><<<sweep_grid(n, D.E1, D.n, 128), 128, 0, s>>>(D, B, X.status,
-                                                                          a);
+      k_face_velocity<0, T><<<tile_grid(n, D.E1, D.n, t), tile_block(t), 0, s>>>(
+          D, B, X.status, a, a + n);
     if (clamp_range(D.g, D.g + D.nr, i0, i1, &a, &n))  // e=0, a=1, bb=2
-      k_face_velocity<1, T><<<sweep_grid(n, D.n + 1, D.E2, 128), 128, 0, s>>>(
-          D, B, X.status, a);
+      k_face_velocity<1, T><<<tile_grid(n, D.n + 1, D.E2, t), tile_block(t), 0, s>>>(
+          D, B, X.status, a, a + n);
     if (clamp_range(0, D.E0, i0, i1, &a, &n))  // e=1, a=2, bb=0 (all i)
-      k_face_velocity<2, T><<<sweep_grid(n, D.n, D.n + 1, 128), 128, 0, s>>>(
-          D, B, X.status, a);
+      k_face_velocity<2, T><<<tile_grid(n, D.n, D.n + 1, t), tile_block(t), 0, s>>>(
+          D, B, X.status, a, a + n);
   }
   static void edge(const Ctx &X, const Bulk<T> &B, const Opts &O, int i0, int i1,
                    cudaStream_t s) {
     const Dims &D = X.D;
     int a, n;
+    const Tile t = X.tile[kTileEdgeEmf];
     if (clamp_range(D.g, D.g + D.nr, i0, i1, &a, &n))
-      k_edge_emf<0, T><<<sweep_grid(n, D.n + 1, D.n + 1, 128), 128, 0, s>>>(
-          D, X.S, X.G, B, O, X.params, X.status, a);
+      k_edge_emf<0, T><<<tile_grid(n, D.n + 1, D.n + 1, t), tile_block(t), 0, s>>>(
+          D, X.S, X.G, B, O, X.params, X.status, a, a + n);
     if (clamp_range(D.g, D.g + D.nr + 1, i0, i1, &a, &n))
-      k_edge_emf<1, T><<<sweep_grid(n, D.n, D.n + 1, 128), 128, 0, s>>>(
-          D, X.S, X.G, B, O, X.params, X.status, a);
+      k_edge_emf<1, T><<<tile_grid(n, D.n, D.n + 1, t), tile_block(t), 0, s>>>(
+          D, X.S, X.G, B, O, X.params, X.status, a, a + n);
     if (clamp_range(D.g, D.g + D.nr + 1, i0, i1, &a, &n))
-      k_edge_emf<2, T><<<sweep_grid(n, D.n + 1, D.n, 128), 128, 0, s>>>(
-          D, X.S, X.G, B, O, X.params, X.status, a);
+      k_edge_emf<2, T><<<tile_grid(n, D.n + 1, D.n, t), tile_block(t), 0, s>>>(
+          D, X.S, X.G, B, O, X.params, X.status, a, a + n);
   }
 };
 

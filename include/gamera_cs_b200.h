@@ -379,6 +379,106 @@ int gcs_context_precision(const gcs_context *ctx);
 int gcs_context_set_bulk_threshold(gcs_context *ctx, double b0_threshold);
 int gcs_context_bulk_split(const gcs_context *ctx);
 
+/* Upstream solar wind of a wind run (no reference counterpart; the
+ * reference driver fixes it at n = 5 cm^-3, V = -400 km/s, T = 1e5 K,
+ * Bz = -5 nT, test_cubedsphere_dipole_background.c:282-294): density
+ * (proton cm^-3, before the seeded +-1% noise), Vx (km/s), proton
+ * temperature (K), IMF Bz (nT). */
+typedef struct gcs_wind_driver {
+  double density_cm3;
+  double velocity_x_kms;
+  double temperature_k;
+  double bz_nt;
+} gcs_wind_driver;
+
+/* The wind case (gcs_context_create_case kind 2: log-stretched r in
+ * [2.5, 30] R_E, aligned dipole, seeded +-1% density noise) with the given
+ * upstream driver. */
+gcs_context *gcs_context_create_wind(size_t nr, size_t n, unsigned long long seed,
+                                     const gcs_wind_driver *driver);
+
+/* Launch tiles (no reference counterpart).  A kernel family's thread block
+ * is a tile of bx consecutive points of the flattened (j, k) plane of a
+ * radial layer times by radial layers; bx * by must be a multiple of 32 and
+ * at most gcs_tile_limit(family).  Tiles change speed, never results.
+ * Defaults: 128 x 1 (recovery/CFL 256 x 1). */
+enum {
+  GCS_TILE_PREDICT = 0,
+  GCS_TILE_FLUX = 1,
+  GCS_TILE_FACE_VELOCITY = 2,
+  GCS_TILE_EDGE_EMF = 3,
+  GCS_TILE_CT = 4,
+  GCS_TILE_UPDATE = 5,
+  GCS_TILE_RECOVER = 6,
+  GCS_TILE_FAMILIES = 7
+};
+int gcs_tile_limit(int family);
+int gcs_context_set_tile(gcs_context *ctx, int family, int bx, int by);
+int gcs_context_tile(const gcs_context *ctx, int family, int *bx, int *by);
+/* Autotuner: for the predictor, flux, face-velocity, edge-EMF and
+ * recovery/CFL families, times every candidate tile (`repetitions`
+ * launches each, CUDA events on the context stream) on the context's
+ * current state and keeps the fastest.  These kernels write only per-step
+ * scratch, so the state is unchanged; CT and the cell update keep their
+ * tile.  best_ms / default_ms (nullable, GCS_TILE_FAMILIES entries, 0 for
+ * untuned families) receive the chosen and the default tile's ms per
+ * launch sequence.  Needs a context with a background (wind case). */
+int gcs_context_autotune(gcs_context *ctx, const gamera_no_advance_options *options,
+                         const gamera_no_timestep_options *timestep, int repetitions,
+                         double best_ms[GCS_TILE_FAMILIES],
+                         double default_ms[GCS_TILE_FAMILIES]);
+
+/* Ensembles (no reference counterpart): independent wind runs of uneven
+ * resolution and different drivers advanced together, one CUDA graph per
+ * ensemble step, each run with its own device time step
+ * (dt = min(dt_fraction * CFL step, 1.25 dt_prev), as gcs_context_run) and
+ * failure status.  Runs of equal (nr, n) share the grid (geometry,
+ * background, plans, FP32 metric, per-step scratch) of the first run of
+ * that size and own only their state; they run one after another inside
+ * the step, runs of different sizes concurrently.  Run i uses the noise
+ * seed `seed + i` and the options of gcs_case_options(2). */
+typedef struct gcs_ensemble gcs_ensemble;
+typedef struct gcs_ensemble_config {
+  int count;
+  const size_t *nr;                 /* radial active cells per run */
+  const size_t *n;                  /* angular active cells per run */
+  const gcs_wind_driver *drivers;   /* one per run */
+  unsigned long long seed;
+  int fp32_bulk;                    /* FP32-bulk sweeps for every run */
+  int autotune_repetitions;         /* 0: default tiles; else tune each grid */
+  double dt_fraction;               /* 0.5 in the reference driver */
+} gcs_ensemble_config;
+/* Seeded draw of `count` runs: angular size from {48, 64, 96, 128} (the
+ * radial size is the caller's; 2n in the ensemble benchmark) and drivers
+ * uniform in Bz [-10, 5] nT, Vx [-800, -300] km/s, n [1, 20] cm^-3,
+ * T [5e4, 2e5] K.  Either output may be NULL. */
+int gcs_ensemble_draw(unsigned long long seed, int count, size_t *n,
+                      gcs_wind_driver *drivers);
+/* Device bytes an ensemble of these sizes needs (host arithmetic). */
+double gcs_ensemble_estimate_bytes(int count, const size_t *nr, const size_t *n,
+                                   int fp32_bulk);
+/* NULL on failure (gcs_last_error(); also when the estimate exceeds the
+ * free device memory). */
+gcs_ensemble *gcs_ensemble_create(const gcs_ensemble_config *config);
+void gcs_ensemble_destroy(gcs_ensemble *ensemble);
+int gcs_ensemble_count(const gcs_ensemble *ensemble);
+/* Run i's context (borrowed; for state downloads, parameters, failures). */
+gcs_context *gcs_ensemble_run_context(gcs_ensemble *ensemble, int run);
+/* Index of the run whose grid run i uses (i itself for the first run of a
+ * size). */
+int gcs_ensemble_grid_owner(const gcs_ensemble *ensemble, int run);
+/* Enqueue `steps` ensemble steps (graph launches) on the ensemble stream;
+ * the first call sets every run's first step size and captures the graph.
+ * Does not synchronise. */
+int gcs_ensemble_advance(gcs_ensemble *ensemble, int steps);
+/* Wait, then check every run's status; *failed_run = first failed run or
+ * -1. */
+int gcs_ensemble_sync(gcs_ensemble *ensemble, int *failed_run);
+uintptr_t gcs_ensemble_stream(gcs_ensemble *ensemble);
+size_t gcs_ensemble_device_bytes(const gcs_ensemble *ensemble);
+/* Nodes of the captured step graph and number of distinct grids. */
+int gcs_ensemble_graph_info(const gcs_ensemble *ensemble, int *nodes, int *grids);
+
 /* Device-resident ionosphere solves (no reference counterpart).  A plan
  * holds `count` independent systems on one polar grid (for example the two
  * hemispheres, configs differing in `hemisphere`); one solve launch runs

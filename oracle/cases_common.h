@@ -44,6 +44,23 @@ static inline double case_wind_pressure(void) {
   return 5.0e6 * 1.380649e-23 * 1.0e5 / (CASE_RHO_NORM * 1.0e10);
 }
 
+/* An explicit upstream driver (n in cm^-3, Vx in km/s, T in K, Bz in nT)
+ * in code units: the density before noise, Vx, pressure n k T and Bz.  No
+ * reference counterpart: the reference driver fixes the values above. */
+typedef struct {
+  double rho, vx, pres, bz;
+} case_driver;
+
+static inline case_driver case_driver_code_units(double density_cm3, double vx_kms,
+                                                 double temperature_k, double bz_nt) {
+  case_driver d;
+  d.rho = density_cm3;
+  d.vx = vx_kms / 100.0;
+  d.pres = density_cm3 * 1.0e6 * 1.380649e-23 * temperature_k / (CASE_RHO_NORM * 1.0e10);
+  d.bz = bz_nt * 1.0e-9 / case_magnetic_norm_tesla();
+  return d;
+}
+
 static inline double case_wind_density(int kind, unsigned long long seed,
                                        int face, size_t cell, double x) {
   double rho = 5.0 * (1.0 + 0.01 * case_noise(seed, face, cell));

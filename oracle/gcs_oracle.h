@@ -90,6 +90,11 @@ int gcso_mi_solve_conductance_tensor(const gamera_mi_solver_config *config,
  * default), noise seed. */
 gcso_case *gcso_case_create(int kind, size_t nr, size_t n,
                             unsigned long long seed);
+/* The wind case with an explicit upstream driver (n cm^-3, Vx km/s, T K,
+ * Bz nT). */
+gcso_case *gcso_case_create_driven(size_t nr, size_t n, unsigned long long seed,
+                                   double density_cm3, double vx_kms,
+                                   double temperature_k, double bz_nt);
 void gcso_case_destroy(gcso_case *c);
 gamera_no_grid *gcso_case_grid(gcso_case *c);
 gamera_no_storage *gcso_case_storage(gcso_case *c);

@@ -32,6 +32,9 @@ def lib():
         for name, res, args in [
                 ("gcso_case_create", C.c_void_p, [C.c_int, C.c_size_t, C.c_size_t,
                                                   C.c_ulonglong]),
+                ("gcso_case_create_driven", C.c_void_p,
+                 [C.c_size_t, C.c_size_t, C.c_ulonglong, C.c_double, C.c_double,
+                  C.c_double, C.c_double]),
                 ("gcso_case_destroy", None, [C.c_void_p]),
                 ("gcso_case_grid", P(abi.Grid), [C.c_void_p]),
                 ("gcso_case_storage", P(abi.Storage), [C.c_void_p]),
@@ -81,11 +84,17 @@ def lib():
 class Case:
     """A six-face case built and advanced by the restatement oracle."""
 
-    def __init__(self, kind, nr=0, n=0, seed=1):
+    def __init__(self, kind, nr=0, n=0, seed=1, driver=None):
+        """driver: (density cm^-3, Vx km/s, T K, Bz nT) of a wind case."""
         if isinstance(kind, str):
             kind = KINDS[kind]
         self.lib = lib()
-        self.handle = self.lib.gcso_case_create(kind, nr, n, seed)
+        if driver is not None:
+            if kind != KINDS["wind"]:
+                raise ValueError("a driver needs the wind case")
+            self.handle = self.lib.gcso_case_create_driven(nr, n, seed, *map(float, driver))
+        else:
+            self.handle = self.lib.gcso_case_create(kind, nr, n, seed)
         if not self.handle:
             raise RuntimeError("oracle case construction failed")
         self.kind = kind

@@ -279,12 +279,20 @@ def run_gpu(args):
 
     mi_solo = run_mi(lib, torch, device, args.mi_solves) if args.mi_solves > 0 else None
     bulk = run_bulk(lib, torch, device, args, dist) if args.bulk else None
+    # the ensemble needs most of the GPU's memory: free the production run first
+    had_mi = mi is not None
+    if mi is not None:
+        lib.gamera_cs_mi_dipole_destroy(mi)
+        mi = None
+    lib.gcs_context_destroy(ctx)
+    ctx = None
+    ens = run_ensemble(lib, torch, device, args, dist, rank) if args.ens_steps > 0 else None
 
     result = None
     if rank == 0:
         clk = clocks.summary()
         launches_per_step = 24
-        mi_updates = 0 if mi is None else -(-args.steps // args.mi_every)
+        mi_updates = 0 if not had_mi else -(-args.steps // args.mi_every)
         result = {
             "metric": METRIC,
             "value": value,
@@ -303,7 +311,7 @@ def run_gpu(args):
                        "faces": 6, "angular": n, "radial": nr,
                        "cells_per_gpu": cells, "ghost": 4,
                        "graph": "one CUDA graph per step, device-side dt",
-                       "mi_coupling": ("none" if mi is None else
+                       "mi_coupling": ("none" if not had_mi else
                                        "every %d steps: shell FAC curl + polar "
                                        "sampling + 2 hemisphere PCG solves, "
                                        "192 x 22 per hemisphere" % args.mi_every),
@@ -336,13 +344,12 @@ def run_gpu(args):
             result["mi"] = mi_solo
         if bulk is not None:
             result["fp32_bulk"] = bulk
+        if ens is not None:
+            result["ensemble"] = ens
         if args.cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(args)
             if mi_solo is not None:
                 result["mi"]["cpu_baseline"] = mi_cpu_baseline()
-    if mi is not None:
-        lib.gamera_cs_mi_dipole_destroy(mi)
-    lib.gcs_context_destroy(ctx)
     if dist is not None:
         dist.destroy_process_group()
     if result is not None:
@@ -392,6 +399,92 @@ def run_bulk(lib, torch, device, args, dist):
             "note": "flux/face-velocity/EMF sweeps in FP32 outside the layers "
                     "where |B0| > 8 (those stay FP64); state, face B, CT, "
                     "predictor and recovery FP64"}
+
+
+ENS_SEED = 2024
+ENS_RUNS = 16
+TILE_FAMILIES = ["predict", "flux", "face_velocity", "edge_emf", "ct", "update",
+                 "recover_cfl"]
+
+
+def run_ensemble(lib, torch, device, args, dist, rank):
+    """Sixteen wind runs drawn from a seed (angular size in {48, 64, 96, 128},
+    radial 2n; upstream n, Vx, T, Bz uniform), FP32-bulk, tiles autotuned per
+    size, advanced together: one CUDA graph per ensemble step, each run with
+    its own device dt.  Value = all runs' active cells x steps / device
+    time of the timed steps (CUDA events on the ensemble stream)."""
+    from gamera_cube_b200 import abi
+    k = ENS_RUNS
+    n = (C.c_size_t * k)()
+    drv = (abi.WindDriver * k)()
+    lib.gcs_ensemble_draw(ENS_SEED, k, n, drv)
+    nr = (C.c_size_t * k)(*[2 * x for x in n])
+    cfg = abi.EnsembleConfig(k, nr, n, drv, ENS_SEED + 100 * rank, 1, 3, 0.5)
+    t0 = time.time()
+    ens = lib.gcs_ensemble_create(C.byref(cfg))
+    if not ens:
+        return {"error": lib.gcs_last_error().decode()}
+    setup_s = time.time() - t0
+    opts, ts = abi.AdvanceOptions(), abi.TimestepOptions()
+    lib.gcs_case_options(KIND_WIND, C.byref(opts), C.byref(ts))
+    tuning = {}
+    for i in range(k):
+        if lib.gcs_ensemble_grid_owner(ens, i) != i:
+            continue
+        ctx = lib.gcs_ensemble_run_context(ens, i)
+        best, dflt = (C.c_double * 7)(), (C.c_double * 7)()
+        lib.gcs_context_autotune(ctx, C.byref(opts), C.byref(ts), 3, best, dflt)
+        tiles = {}
+        for f, name in enumerate(TILE_FAMILIES):
+            bx, by = C.c_int(), C.c_int()
+            lib.gcs_context_tile(ctx, f, C.byref(bx), C.byref(by))
+            tiles[name] = [bx.value, by.value]
+        tuning["%dx%dx%d" % (n[i], n[i], nr[i])] = {
+            "tiles": tiles, "tuned_ms": round(sum(best), 4),
+            "default_ms": round(sum(dflt), 4)}
+    stream = torch.cuda.ExternalStream(lib.gcs_ensemble_stream(ens), device=device)
+    failed = C.c_int()
+    ok = lib.gcs_ensemble_advance(ens, args.ens_warmup) == 0 and \
+        lib.gcs_ensemble_sync(ens, C.byref(failed)) == 0
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    start.record(stream)
+    ok = ok and lib.gcs_ensemble_advance(ens, args.ens_steps) == 0
+    stop.record(stream)
+    stop.synchronize()
+    ok = ok and lib.gcs_ensemble_sync(ens, C.byref(failed)) == 0
+    torch.cuda.synchronize()
+    barrier(dist, device)
+    ms = max_over_ranks(start.elapsed_time(stop), dist, device)
+    cells_local = sum(6 * nr[i] * n[i] * n[i] for i in range(k))
+    cells = sum_over_ranks(float(cells_local), dist, device)
+    nodes, grids = C.c_int(), C.c_int()
+    lib.gcs_ensemble_graph_info(ens, C.byref(nodes), C.byref(grids))
+    dts = []
+    for i in range(k):
+        dt, st = C.c_double(), C.c_int()
+        lib.gcs_context_params(lib.gcs_ensemble_run_context(ens, i), C.byref(dt), None,
+                               None, C.byref(st))
+        dts.append(dt.value)
+    out = {"value": cells * args.ens_steps / (ms * 1e-3), "unit": "cell-updates/s",
+           "ms_per_ensemble_step": ms / args.ens_steps,
+           "steps": args.ens_steps, "warmup": args.ens_warmup,
+           "all_runs_ok": bool(ok), "failed_run": failed.value,
+           "projected_500_steps_s": ms / args.ens_steps * 500 * 1e-3,
+           "workload": "16 wind runs, seed %d: angular sizes %s, radial 2n, FP32-bulk, "
+                       "drivers n [1,20] cm^-3, Vx [-800,-300] km/s, T [5e4,2e5] K, "
+                       "Bz [-10,5] nT" % (ENS_SEED, sorted(list(n))),
+           "cells_per_gpu": cells_local, "grids": grids.value,
+           "graph": "one CUDA graph per ensemble step, %d kernel nodes; one branch per "
+                    "grid size, runs of a size in sequence" % nodes.value,
+           "gpu_launches": nodes.value * args.ens_steps,
+           "device_bytes": lib.gcs_ensemble_device_bytes(ens),
+           "setup_s": round(setup_s, 2),
+           "dt_range": [min(dts), max(dts)],
+           "autotune": tuning}
+    lib.gcs_ensemble_destroy(ens)
+    return out
 
 
 MI_GRID = (361, 181)            # longitudes, colatitudes per hemisphere
@@ -686,6 +779,9 @@ def main():
                     help="timed ionosphere solves (0 skips the MI measurement)")
     ap.add_argument("--no-bulk", dest="bulk", action="store_false",
                     help="skip the FP32-bulk variant measurement")
+    ap.add_argument("--ens-steps", type=int, default=20,
+                    help="timed steps of the 16-run ensemble (0 skips it)")
+    ap.add_argument("--ens-warmup", type=int, default=3)
     ap.add_argument("--only-mi", action="store_true",
                     help="run only the standalone ionosphere solve measurement "
                          "(prints its JSON object; for profiling)")

@@ -218,6 +218,30 @@ class MiAnalysisView(C.Structure):
                 ("potential_v", C.POINTER(C.c_double) * 2)]
 
 
+class SolarWindState(C.Structure):
+    """nonorthogonal/src/solar_wind.h:17-22"""
+    _fields_ = [("density", C.c_double), ("pressure", C.c_double),
+                ("velocity", C.c_double * 3), ("magnetic", C.c_double * 3)]
+
+
+class SolarWindSeries(C.Structure):
+    """nonorthogonal/src/solar_wind.h:24-35"""
+    _fields_ = [("count", C.c_size_t), ("time", C.POINTER(C.c_double)),
+                ("state", C.POINTER(SolarWindState)), ("reference", C.c_double * 3),
+                ("time_offset", C.c_double), ("by_coefficient", C.c_double),
+                ("bz_coefficient", C.c_double), ("bx_offset", C.c_double),
+                ("enforce_bx_relation", C.c_int), ("linear_interpolation", C.c_int)]
+
+
+class EarthBoundary(C.Structure):
+    """cubedsphere/cubedsphere_earth_boundary.h:13-24"""
+    _fields_ = [("startup", C.POINTER(EarthStartup)), ("wind", C.POINTER(SolarWindSeries)),
+                ("background", C.POINTER(BackgroundField)), ("mi", C.c_void_p),
+                ("density_floor", C.c_double), ("pressure_floor", C.c_double),
+                ("step_time", C.c_double), ("step_dt", C.c_double), ("cfl", C.c_double),
+                ("strict_inner_gas_wall", C.c_int)]
+
+
 class WindDriver(C.Structure):
     """gcs_wind_driver: upstream n (cm^-3), Vx (km/s), T (K), IMF Bz (nT)."""
     _fields_ = [("density_cm3", C.c_double), ("velocity_x_kms", C.c_double),
@@ -257,6 +281,14 @@ def ensemble_signatures():
         "gcs_ensemble_stream": (C.c_size_t, [C.c_void_p]),
         "gcs_ensemble_device_bytes": (C.c_size_t, [C.c_void_p]),
         "gcs_ensemble_graph_info": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int)]),
+        "gcs_earth_create": (C.c_int, [C.c_void_p, P(Grid), P(EarthBoundary),
+                                       P(C.c_void_p)]),
+        "gcs_earth_set_wind": (C.c_int, [C.c_void_p, P(SolarWindSeries)]),
+        "gcs_earth_destroy": (None, [C.c_void_p]),
+        "gcs_earth_device_bytes": (C.c_size_t, [C.c_void_p]),
+        "gcs_context_step_earth": (C.c_int, [C.c_void_p, C.c_void_p, P(AdvanceOptions),
+                                             C.c_double, C.c_double, C.c_double,
+                                             C.c_double]),
     }
 
 

@@ -2,6 +2,7 @@
 // device-resident context API declared in include/gamera_cs_b200.h.
 #include "gamera_cs_b200.h"
 #include "gcs_context.h"
+#include "gcs_earth.h"
 
 #include <cfloat>
 #include <cmath>
@@ -218,7 +219,7 @@ bool device_failed(gcs::Context &C) {
 // The stage sequence of one step (cubedsphere_step.c:48-152).  With hooks,
 // host callbacks run at their reference positions on downloaded arrays.
 int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
-             const Hooks *hk) {
+             const Hooks *hk, const gcs::EarthStep *es = nullptr) {
   gcs::Context &C = ctx->c;
   if (hk && C.X.bulk &&
       (hk->radial || hk->options->fluid_flux_sync || hk->options->edge_emf_sync)) {
@@ -232,6 +233,7 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   gcs::launch_seam_sync(X, 1, s);
   mk.mark(kSlotSeamPhi);
   gcs::launch_halo(X, s);
+  if (es) gcs::launch_earth_radial(X, *es->dev, es->current_time, es->previous_time, s);
   mk.mark(kSlotHalo);
   const size_t lower[3] = {hk ? hk->ghost : 0, hk ? hk->ghost : 0,
                            hk ? hk->ghost : 0};
@@ -250,6 +252,7 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   gcs::launch_flux(X, O, s);
   mk.mark(kSlotFlux);
   gcs::launch_seam_sync(X, 0, s);
+  if (es) gcs::launch_earth_trap(X, s);
   mk.mark(kSlotSeamFlux);
   if (hk && hk->options->fluid_flux_sync) {
     if (device_failed(C) || transfer_fluxes(C, hk->storage, false) != 0)
@@ -262,6 +265,7 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   }
   if (O.u_mhd) {
     gcs::launch_emf(X, O, s);
+    if (es) gcs::launch_earth_emf(X, *es->dev, es->step_time, es->step_dt, s);
     mk.mark(kSlotEmf);
     if (hk && hk->options->edge_emf_sync) {
       if (device_failed(C) || transfer_emf(C, hk->storage, false) != 0)
@@ -942,6 +946,36 @@ int gcs_context_step(gcs_context *ctx, const gamera_no_advance_options *options,
     return -1;
   C.reset_status_async();
   const int rc = run_step(ctx, O, 0, nullptr);
+  const bool fail = device_failed(C);
+  if (fail) report_failure(C);
+  return (rc != 0 || fail) ? -1 : 0;
+}
+
+int gcs_context_step_earth(gcs_context *ctx, gcs_earth *earth,
+                           const gamera_no_advance_options *options,
+                           double ratio, double dt, double current_time,
+                           double previous_time) {
+  if (!ctx || !earth || earth->ctx != ctx || !options) return -1;
+  if (!std::isfinite(current_time) || !std::isfinite(previous_time) || !(dt > 0.0) ||
+      !std::isfinite(dt)) {
+    set_last("invalid step times");
+    return -1;
+  }
+  gcs::Opts O;
+  if (!make_opts(options, ctx->c.bg_uploaded != 0, &O)) return -1;
+  gcs::Context &C = ctx->c;
+  gcs::StepParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.dt = dt;
+  p.ratio = ratio;
+  if (cudaMemcpyAsync(C.X.params, &p, sizeof(p), cudaMemcpyHostToDevice,
+                      C.stream) != cudaSuccess)
+    return -1;
+  C.reset_status_async();
+  // the reference driver sets step_time = current time, step_dt = dt
+  // (test_cubedsphere_dipole_background.c:667-668)
+  const gcs::EarthStep es{&earth->dev, current_time, previous_time, current_time, dt};
+  const int rc = run_step(ctx, O, 0, nullptr, &es);
   const bool fail = device_failed(C);
   if (fail) report_failure(C);
   return (rc != 0 || fail) ? -1 : 0;

@@ -1,0 +1,664 @@
+// Device Earth radial boundary (no-MI wall) for the six-face step: the
+// reference callbacks gamera_cs_earth_fill_radial_ghosts,
+// gamera_cs_earth_inner_fluid_flux and gamera_cs_earth_no_mi_emf
+// (cubedsphere/cubedsphere_earth_boundary.c) and the solar-wind sampling
+// they call (nonorthogonal/src/solar_wind.c), restated as kernels with the
+// reference's operation order.  One thread per boundary cell, face or edge;
+// all six faces in one launch.  A failure (invalid state, wind sample or
+// area) records the host-callback stage, as the reference callback's -1
+// fails the step.
+#include "gcs_context.h"
+#include "gcs_earth.h"
+#include "gcs_error.h"
+#include "gamera_cs_b200.h"
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "gcs_kernel_util.cuh"
+#include "gcs_physics.cuh"
+
+namespace gcs {
+namespace {
+
+struct WindState {
+  double rho, p, v[3], b[3];
+};
+
+__device__ inline WindState wind_load(const WindDev &w, int q) {
+  const double *a = w.state + 8LL * q;
+  WindState s;
+  s.rho = a[0];
+  s.p = a[1];
+  for (int c = 0; c < 3; ++c) {
+    s.v[c] = a[2 + c];
+    s.b[c] = a[5 + c];
+  }
+  return s;
+}
+
+// solar_wind.c:8-22
+__device__ inline bool wind_finite(const WindState &s) {
+  if (!isfinite(s.rho) || !isfinite(s.p) || s.rho <= 0.0 || s.p <= 0.0) return false;
+  for (int c = 0; c < 3; ++c)
+    if (!isfinite(s.v[c]) || !isfinite(s.b[c])) return false;
+  return fabs(s.v[0]) > DBL_MIN;
+}
+
+// solar_wind.c:134-160 (binary search of :104-117, interpolation :119-132)
+__device__ bool wind_sample_time(const WindDev &w, double time, WindState *out) {
+  if (!isfinite(time)) return false;
+  if (w.count == 1 || time <= w.time[0]) {
+    *out = wind_load(w, 0);
+    return true;
+  }
+  if (time >= w.time[w.count - 1]) {
+    *out = wind_load(w, w.count - 1);
+    return true;
+  }
+  int lo = 0, hi = w.count - 1;
+  while (hi - lo > 1) {
+    const int mid = lo + (hi - lo) / 2;
+    if (w.time[mid] <= time)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const WindState a = wind_load(w, lo);
+  if (!w.linear) {
+    *out = a;
+    return true;
+  }
+  const WindState z = wind_load(w, lo + 1);
+  const double fr = (time - w.time[lo]) / (w.time[lo + 1] - w.time[lo]);
+  out->rho = a.rho + fr * (z.rho - a.rho);
+  out->p = a.p + fr * (z.p - a.p);
+  for (int c = 0; c < 3; ++c) {
+    out->v[c] = a.v[c] + fr * (z.v[c] - a.v[c]);
+    out->b[c] = a.b[c] + fr * (z.b[c] - a.b[c]);
+  }
+  return wind_finite(*out);
+}
+
+// Planar-front ballistic mapping, solar_wind.c:162-200.
+__device__ bool wind_sample_at(const WindDev &w, const double x[3], double t,
+                               WindState *out) {
+  if (!isfinite(t)) return false;
+  const double monitor = t + w.time_offset;
+  WindState cur;
+  if (!wind_sample_time(w, monitor, &cur)) return false;
+  const double csq = w.by * w.by + w.bz * w.bz;
+  const double factor = cur.v[0] / (1.0 + csq);
+  const double fv[3] = {factor, -factor * w.by, -factor * w.bz};
+  double s2 = 0.0, proj = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    if (!isfinite(x[c])) return false;
+    s2 += fv[c] * fv[c];
+    proj += (x[c] - w.reference[c]) * fv[c];
+  }
+  if (!(s2 > DBL_MIN) || !isfinite(s2)) return false;
+  const double delay = proj / s2;
+  return wind_sample_time(w, monitor - delay, out);
+}
+
+// Upstream-to-tail weight, solar_wind.c:202-225, on the state the mapping
+// returns for the same point and time.
+__device__ bool wind_weight(const double x[3], const WindState &s, double *weight) {
+  double r2 = 0.0, v2 = 0.0, cosine = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    r2 += x[c] * x[c];
+    v2 += s.v[c] * s.v[c];
+    cosine -= x[c] * s.v[c];
+  }
+  if (!(r2 > DBL_MIN) || !(v2 > DBL_MIN)) return false;
+  cosine /= sqrt(r2 * v2);
+  cosine = fmax(-1.0, fmin(1.0, cosine));
+  const double angle = acos(cosine);
+  const double half_pi = 0.5 * acos(-1.0);
+  if (angle <= half_pi) {
+    *weight = 1.0;
+  } else if (angle >= 2.0 * half_pi) {
+    *weight = 0.0;
+  } else {
+    const double sc = (angle - half_pi) / half_pi;
+    *weight = exp(1.0 - 1.0 / (1.0 - sc * sc));
+  }
+  return true;
+}
+
+// cubedsphere_earth_boundary.c:16-25
+__device__ inline bool sample_wind(const WindDev &w, const double x[3], double t,
+                                   WindState *s, double *weight) {
+  return wind_sample_at(w, x, t, s) && wind_weight(x, *s, weight);
+}
+
+__device__ inline long long plane(const Dims &D, int f, int layers, int l, int j, int k) {
+  return (((long long)f * layers + l) * D.N1 + j) * D.N2 + k;
+}
+
+// Radial ghost cells of U (old = 0) or U_old (old = 1),
+// cubedsphere_earth_boundary.c:27-112: inner ghosts mirror the first active
+// layers with the normal velocity reversed (or zero velocity on the strict
+// wall); outer ghosts take the last active cell, raise a subsonic outward
+// velocity to the sound speed and blend with the sampled wind.
+__global__ void k_earth_cells(Dims D, DevState S, EarthDev E, double time, int old,
+                              DevStatus *st) {
+  if (failed(st)) return;
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= D.E1 * D.E2) return;
+  const int l = blockIdx.y, f = blockIdx.z;
+  const int j = jk / D.E2, k = jk % D.E2;
+  const int outer = D.g + D.nr;
+  const bool inner = l < D.g;
+  const int i = inner ? l : outer + (l - D.g);
+  const int si = inner ? 2 * D.g - 1 - i : outer - 1;
+  double *const *U = old ? S.Uo : S.U;
+  const long long src = f * D.Nn + D.node(si, j, k);
+  const long long dst = f * D.Nn + D.node(i, j, k);
+  double u[5];
+  for (int m = 0; m < 5; ++m) u[m] = U[m][src];
+  Prim p;
+  if (cons_to_prim(u, E.gamma, E.rho_floor, E.p_floor, &p)) {
+    fail(st, kStageHost, 0, f, i, j, k);
+    return;
+  }
+  const long long q = plane(D, f, 2 * D.g, l, j, k);
+  const double x[3] = {E.cell_cen[0][q], E.cell_cen[1][q], E.cell_cen[2][q]};
+  const double radius = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  if (!(radius > 0.0)) {
+    fail(st, kStageHost, 0, f, i, j, k);
+    return;
+  }
+  double v[3] = {p.vx, p.vy, p.vz};
+  if (inner) {
+    if (E.strict_wall) {
+      v[0] = v[1] = v[2] = 0.0;
+    } else {
+      double vn = 0.0;
+      for (int c = 0; c < 3; ++c) vn += v[c] * x[c] / radius;
+      for (int c = 0; c < 3; ++c) v[c] -= 2.0 * vn * x[c] / radius;
+    }
+  } else {
+    WindState w;
+    double wt;
+    if (!sample_wind(E.wind, x, time, &w, &wt)) {
+      fail(st, kStageHost, 0, f, i, j, k);
+      return;
+    }
+    double vn = 0.0;
+    for (int c = 0; c < 3; ++c) vn += v[c] * x[c] / radius;
+    const double cs = sqrt(E.gamma * p.p / p.rho);
+    if (vn < cs)
+      for (int c = 0; c < 3; ++c) v[c] += (cs - vn) * x[c] / radius;
+    p.rho = wt * w.rho + (1.0 - wt) * p.rho;
+    p.p = wt * w.p + (1.0 - wt) * p.p;
+    for (int c = 0; c < 3; ++c) v[c] = wt * w.v[c] + (1.0 - wt) * v[c];
+  }
+  p.vx = v[0];
+  p.vy = v[1];
+  p.vz = v[2];
+  double out[5];
+  if (prim_to_cons(p, E.gamma, E.rho_floor, E.p_floor, out)) {
+    fail(st, kStageHost, 0, f, i, j, k);
+    return;
+  }
+  for (int m = 0; m < 5; ++m) U[m][dst] = out[m];
+}
+
+// Radial ghost faces of family d, cubedsphere_earth_boundary.c:114-163:
+// inner ghosts carry the first active face's flux density; outer ghosts
+// blend the wind's residual flux (B_wind . area vector - B0 flux) with the
+// last face inside.
+__global__ void k_earth_faces(Dims D, DevState S, DevGeom G, EarthDev E, int d,
+                              double time, int old, DevStatus *st) {
+  if (failed(st)) return;
+  const int e1 = D.E1 + (d == 1), e2 = D.E2 + (d == 2);
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= e1 * e2) return;
+  const int l = blockIdx.y, f = blockIdx.z;
+  const int j = jk / e2, k = jk % e2;
+  const int outer = D.g + D.nr;
+  double *P = old ? S.Po[d] : S.P[d];
+  if (l < D.g) {
+    const int i = l;
+    const long long c = f * D.Nn + D.node(i, j, k);
+    const long long src = f * D.Nn + D.node(D.g, j, k);
+    const double sa = G.area[d][src];
+    if (!(sa > 0.0)) {
+      fail(st, kStageHost, d, f, i, j, k);
+      return;
+    }
+    P[c] = P[src] * G.area[d][c] / sa;
+    return;
+  }
+  const int lo = l - D.g;
+  const int i = outer + (d == 0) + lo;
+  const long long q = plane(D, f, D.g, lo, j, k);
+  const double x[3] = {E.face_cen[d][0][q], E.face_cen[d][1][q], E.face_cen[d][2][q]};
+  WindState w;
+  double wt;
+  if (!sample_wind(E.wind, x, time, &w, &wt)) {
+    fail(st, kStageHost, d, f, i, j, k);
+    return;
+  }
+  double wf = -E.face_bg[d][q];
+  for (int c = 0; c < 3; ++c) wf += w.b[c] * E.face_av[d][c][q];
+  const int si = d == 0 ? outer : outer - 1;
+  const long long c = f * D.Nn + D.node(i, j, k);
+  P[c] = wt * wf + (1.0 - wt) * P[f * D.Nn + D.node(si, j, k)];
+}
+
+// Cell B (old = 0) or old cell B (old = 1) of every cell from the face
+// fluxes (nonorthogonal_step.c:310-358 as called at
+// cubedsphere_earth_boundary.c:169-172).
+__global__ void k_earth_recover(Dims D, DevState S, DevGeom G, int old, DevStatus *st) {
+  if (failed(st)) return;
+  int f, i, j, k;
+  const Box b{0, 0, 0, D.E1, D.E2, D.E0};
+  if (!box_coord(b, &f, &i, &j, &k)) return;
+  const long long c = f * D.Nn + D.node(i, j, k);
+  double *const *P = old ? S.Po : S.P;
+  double phi[6], bn[3];
+  const long long sdir[3] = {D.stride(0), D.stride(1), 1};
+  for (int d = 0; d < 3; ++d) {
+    phi[2 * d] = P[d][c];
+    phi[2 * d + 1] = P[d][c + sdir[d]];
+  }
+  if (!recover_cell(G, c, phi, bn)) {
+    fail(st, kStageHost, 0, f, i, j, k);
+    return;
+  }
+  double *const *B = old ? S.Bo : S.B;
+  for (int m = 0; m < 3; ++m) B[m][c] = bn[m];
+}
+
+// dB/dr = 0 in the inner ghost cells (cubedsphere_earth_boundary.c:173-182).
+__global__ void k_earth_copy_inner(Dims D, DevState S, int old) {
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= D.E1 * D.E2) return;
+  const int i = blockIdx.y, f = blockIdx.z;
+  const int j = jk / D.E2, k = jk % D.E2;
+  double *const *B = old ? S.Bo : S.B;
+  const long long src = f * D.Nn + D.node(D.g, j, k);
+  const long long dst = f * D.Nn + D.node(i, j, k);
+  for (int m = 0; m < 3; ++m) B[m][dst] = B[m][src];
+}
+
+// No outward mass (and then energy) flux through the inner shell,
+// nonorthogonal_step.c:35-72 as called at cubedsphere_earth_boundary.c:259-266.
+__global__ void k_earth_trap(Dims D, DevState S) {
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= D.n * D.n) return;
+  const int f = blockIdx.z;
+  const int j = D.g + jk / D.n, k = D.g + jk % D.n;
+  const long long c = f * D.Nn + D.node(D.g, j, k);
+  if (S.F[0][0][c] > 0.0) {
+    S.F[0][0][c] = 0.0;
+    if (S.F[0][4][c] > 0.0) S.F[0][4][c] = 0.0;
+  }
+}
+
+// Outer edges of family d in the last four layers up to the outer shell:
+// blend the EMF with the wind's -v x B line integral, the weight falling as
+// 1 / (1 + layers inside), cubedsphere_earth_boundary.c:390-425.
+__global__ void k_earth_emf_outer(Dims D, DevState S, EarthDev E, int d, double tmid,
+                                  DevStatus *st) {
+  if (failed(st)) return;
+  const int e1 = D.E1 + (d != 1), e2 = D.E2 + (d != 2);
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= e1 * e2) return;
+  const int l = 1 + blockIdx.y, f = blockIdx.z;
+  const int j = jk / e2, k = jk % e2;
+  const int outer = D.g + D.nr;
+  const int i = outer - 3 + (l - 1);
+  const long long q = plane(D, f, 5, l, j, k);
+  if (!E.edge_valid[d][q]) return;
+  const double x[3] = {E.edge_mid[d][0][q], E.edge_mid[d][1][q], E.edge_mid[d][2][q]};
+  WindState w;
+  double wt;
+  if (!sample_wind(E.wind, x, tmid, &w, &wt)) {
+    fail(st, kStageHost, d, f, i, j, k);
+    return;
+  }
+  if (i < outer) wt /= 1.0 + (double)(outer - i);
+  const double el[3] = {-(w.v[1] * w.b[2] - w.v[2] * w.b[1]),
+                        -(w.v[2] * w.b[0] - w.v[0] * w.b[2]),
+                        -(w.v[0] * w.b[1] - w.v[1] * w.b[0])};
+  const double len = E.edge_len[d][q];
+  double li = 0.0;
+  for (int c = 0; c < 3; ++c) li += el[c] * E.edge_nrm[d][c][q] * len;
+  const long long c = f * D.Nn + D.node(i, j, k);
+  S.E[d][c] = (1.0 - wt) * S.E[d][c] + wt * li;
+}
+
+__device__ inline bool flux_density(const Dims &D, const DevState &S, const DevGeom &G,
+                                    int f, int d, int i, int j, int k, double *out) {
+  if (i >= D.E0 + (d == 0) || j >= D.E1 + (d == 1) || k >= D.E2 + (d == 2)) return false;
+  const long long c = f * D.Nn + D.node(i, j, k);
+  const double area = G.area[d][c];
+  if (!(area > 0.0)) return false;
+  *out = S.Pp[d][c] / area;
+  return isfinite(*out);
+}
+
+// Wind-front diffusive EMF on the outer shell's j and k edges,
+// cubedsphere_earth_boundary.c:298-379.
+__global__ void k_earth_emf_diffusive(Dims D, DevState S, DevGeom G, EarthDev E,
+                                      double tmid, double dt, DevStatus *st) {
+  if (failed(st)) return;
+  const int w1 = D.n + 1;
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= w1 * w1) return;
+  const int f = blockIdx.z;
+  const int j = D.g + jk / w1, k = D.g + jk % w1;
+  const int i = D.g + D.nr;
+  if (j == 0 || k == 0 || i >= D.E0 + 1 || j >= D.E1 || k >= D.E2 + 1 || j >= D.E1 + 1 ||
+      k >= D.E2)
+    return;
+  const long long qj = plane(D, f, 5, 4, j, k);
+  if (!E.edge_valid[1][qj] || !E.edge_valid[2][qj]) return;
+  double bikp, bikm, bkip, bkim, bjip, bjim, bijp, bijm;
+  if (!flux_density(D, S, G, f, 0, i, j, k, &bikp) ||
+      !flux_density(D, S, G, f, 0, i, j, k - 1, &bikm) ||
+      !flux_density(D, S, G, f, 2, i, j, k, &bkip) ||
+      !flux_density(D, S, G, f, 2, i - 1, j, k, &bkim) ||
+      !flux_density(D, S, G, f, 1, i, j, k, &bjip) ||
+      !flux_density(D, S, G, f, 1, i - 1, j, k, &bjim) ||
+      !flux_density(D, S, G, f, 0, i, j, k, &bijp) ||
+      !flux_density(D, S, G, f, 0, i, j - 1, k, &bijm)) {
+    fail(st, kStageHost, 1, f, i, j, k);
+    return;
+  }
+  const double cur_j = (bikp - bikm) - (bkip - bkim);
+  const double cur_k = (bjip - bjim) - (bijp - bijm);
+  const double dl = sqrt(E.edge_len[1][qj] * E.edge_len[2][qj]);
+  const double xj[3] = {E.edge_mid[1][0][qj], E.edge_mid[1][1][qj], E.edge_mid[1][2][qj]};
+  const double xk[3] = {E.edge_mid[2][0][qj], E.edge_mid[2][1][qj], E.edge_mid[2][2][qj]};
+  WindState wj, wk;
+  double wtj, wtk;
+  if (!(dl > 0.0) || !sample_wind(E.wind, xj, tmid, &wj, &wtj) ||
+      !sample_wind(E.wind, xk, tmid, &wk, &wtk)) {
+    fail(st, kStageHost, 1, f, i, j, k);
+    return;
+  }
+  const double csq = E.wind.by * E.wind.by + E.wind.bz * E.wind.bz;
+  const double front = fmax(fabs(wj.v[0]), fabs(wk.v[0])) / sqrt(1.0 + csq);
+  const double speed = fmin(front, E.cfl * dl / dt);
+  const long long c = f * D.Nn + D.node(i, j, k);
+  S.E[1][c] += wtj * speed * cur_j * dl;
+  S.E[2][c] += wtk * speed * cur_k * dl;
+}
+
+// E_t = 0 on the inner shell (cubedsphere_earth_boundary.c:428-437).
+__global__ void k_earth_emf_inner(Dims D, DevState S, EarthDev E, int d) {
+  const int e1 = D.E1 + (d != 1), e2 = D.E2 + (d != 2);
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= e1 * e2) return;
+  const int f = blockIdx.z;
+  const int j = jk / e2, k = jk % e2;
+  if (!E.edge_valid[d][plane(D, f, 5, 0, j, k)]) return;
+  S.E[d][f * D.Nn + D.node(D.g, j, k)] = 0.0;
+}
+
+inline unsigned blocks(long long n) { return (unsigned)((n + 127) / 128); }
+
+}  // namespace
+
+void launch_earth_radial(const Ctx &X, const EarthDev &E, double current_time,
+                         double previous_time, cudaStream_t s) {
+  const Dims &D = X.D;
+  const dim3 gc(blocks((long long)D.E1 * D.E2), 2 * D.g, kFaces);
+  k_earth_cells<<<gc, 128, 0, s>>>(D, X.S, E, current_time, 0, X.status);
+  k_earth_cells<<<gc, 128, 0, s>>>(D, X.S, E, previous_time, 1, X.status);
+  const Tile t{128, 1};
+  for (int old = 0; old < 2; ++old) {
+    const double time = old ? previous_time : current_time;
+    for (int d = 0; d < 3; ++d) {
+      const long long pl = (long long)(D.E1 + (d == 1)) * (D.E2 + (d == 2));
+      k_earth_faces<<<dim3(blocks(pl), 2 * D.g, kFaces), 128, 0, s>>>(D, X.S, X.G, E, d,
+                                                                       time, old, X.status);
+    }
+    k_earth_recover<<<tile_grid(D.E0, D.E1, D.E2, t), tile_block(t), 0, s>>>(D, X.S, X.G,
+                                                                              old, X.status);
+    k_earth_copy_inner<<<dim3(blocks((long long)D.E1 * D.E2), D.g, kFaces), 128, 0, s>>>(
+        D, X.S, old);
+  }
+}
+
+void launch_earth_trap(const Ctx &X, cudaStream_t s) {
+  k_earth_trap<<<dim3(blocks((long long)X.D.n * X.D.n), 1, kFaces), 128, 0, s>>>(X.D, X.S);
+}
+
+void launch_earth_emf(const Ctx &X, const EarthDev &E, double step_time, double step_dt,
+                      cudaStream_t s) {
+  const Dims &D = X.D;
+  const double tmid = step_time + 0.5 * step_dt;
+  for (int d = 0; d < 3; ++d) {
+    const long long pl = (long long)(D.E1 + (d != 1)) * (D.E2 + (d != 2));
+    k_earth_emf_outer<<<dim3(blocks(pl), 4, kFaces), 128, 0, s>>>(D, X.S, E, d, tmid,
+                                                                   X.status);
+  }
+  k_earth_emf_diffusive<<<dim3(blocks((long long)(D.n + 1) * (D.n + 1)), 1, kFaces), 128, 0,
+                          s>>>(D, X.S, X.G, E, tmid, step_dt, X.status);
+  for (int d = 1; d < 3; ++d) {
+    const long long pl = (long long)(D.E1 + (d != 1)) * (D.E2 + (d != 2));
+    k_earth_emf_inner<<<dim3(blocks(pl), 1, kFaces), 128, 0, s>>>(D, X.S, E, d);
+  }
+}
+
+}  // namespace gcs
+
+namespace {
+
+int upload_wind(gcs_earth *e, const gamera_solar_wind_series *w) {
+  if (!w || w->count < 1 || w->count > (1u << 30) || !w->time || !w->state) {
+    gcs::set_api_error("invalid solar-wind series");
+    return -1;
+  }
+  for (int c = 0; c < 3; ++c)
+    if (!std::isfinite(w->reference[c])) {
+      gcs::set_api_error("invalid solar-wind series");
+      return -1;
+    }
+  const size_t n = w->count;
+  void *pool = nullptr;
+  if (cudaMalloc(&pool, n * 9 * sizeof(double)) != cudaSuccess) {
+    gcs::set_api_error("cannot allocate the solar-wind series");
+    return -1;
+  }
+  std::vector<double> host(n * 9);
+  for (size_t q = 0; q < n; ++q) {
+    host[q] = w->time[q];
+    const gamera_solar_wind_state &s = w->state[q];
+    double *a = &host[n + 8 * q];
+    a[0] = s.density;
+    a[1] = s.pressure;
+    for (int c = 0; c < 3; ++c) {
+      a[2 + c] = s.velocity[c];
+      a[5 + c] = s.magnetic[c];
+    }
+  }
+  if (cudaMemcpy(pool, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice) !=
+      cudaSuccess) {
+    cudaFree(pool);
+    gcs::set_api_error("cannot upload the solar-wind series");
+    return -1;
+  }
+  if (e->wind_pool) cudaFree(e->wind_pool);
+  e->wind_pool = pool;
+  gcs::WindDev &W = e->dev.wind;
+  W.count = (int)n;
+  W.linear = w->linear_interpolation;
+  W.time = (const double *)pool;
+  W.state = (const double *)pool + n;
+  for (int c = 0; c < 3; ++c) W.reference[c] = w->reference[c];
+  W.time_offset = w->time_offset;
+  W.by = w->by_coefficient;
+  W.bz = w->bz_coefficient;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                     const gamera_cs_earth_boundary *b, gcs_earth **out) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (!ctx || !grid || !b || !b->startup || !b->wind || !b->background ||
+      !std::isfinite(b->density_floor) || !(b->density_floor > 0.0) ||
+      !std::isfinite(b->pressure_floor) || !(b->pressure_floor > 0.0) ||
+      !(b->cfl > 0.0) || !std::isfinite(b->startup->gamma)) {
+    gcs::set_api_error("invalid Earth boundary");
+    return -1;
+  }
+  if (b->mi != nullptr && gamera_cs_mi_dipole_ready(b->mi)) {
+    gcs::set_api_error("the MI-coupled inner wall needs the host callback path");
+    return -1;
+  }
+  const gcs::Dims &D = ctx->c.X.D;
+  for (int f = 0; f < gcs::kFaces; ++f) {
+    const gamera_no_grid &g = grid[f];
+    if ((int)g.cell_extent[0] != D.E0 || (int)g.cell_extent[1] != D.E1 ||
+        (int)g.cell_extent[2] != D.E2 || !g.cell || !g.vertex ||
+        !b->background[f].face_flux[0] || !b->background[f].face_flux[1] ||
+        !b->background[f].face_flux[2]) {
+      gcs::set_api_error("grid or background does not match the context");
+      return -1;
+    }
+    for (int d = 0; d < 3; ++d)
+      if (!g.face[d].value || !g.edge[d].value || !g.edge[d].valid) {
+        gcs::set_api_error("grid without face or edge geometry");
+        return -1;
+      }
+  }
+  gcs_earth *e = new (std::nothrow) gcs_earth;
+  if (!e) return -1;
+  e->ctx = ctx;
+  const long long P = (long long)D.N1 * D.N2;
+  const int g = D.g, outer = D.g + D.nr;
+  const long long ncell = 6LL * 2 * g * P, nface = 6LL * g * P, nedge = 6LL * 5 * P;
+  const long long doubles = 3 * ncell + 3 * 7 * nface + 3 * 7 * nedge;
+  std::vector<double> h(doubles, 0.0);
+  std::vector<unsigned char> hv(3 * nedge, 0);
+  double *cell = h.data();
+  double *face = cell + 3 * ncell;
+  double *edge = face + 3 * 7 * nface;
+  auto pl = [&](int f, int layers, int l, int j, int k) {
+    return (((long long)f * layers + l) * D.N1 + j) * D.N2 + k;
+  };
+  for (int f = 0; f < 6; ++f) {
+    const gamera_no_grid &G = grid[f];
+    for (int l = 0; l < 2 * g; ++l) {
+      const int i = l < g ? l : outer + (l - g);
+      for (int j = 0; j < D.E1; ++j)
+        for (int k = 0; k < D.E2; ++k) {
+          const gamera_no_vec3 &x = G.cell[((size_t)i * D.E1 + j) * D.E2 + k].centroid;
+          for (int c = 0; c < 3; ++c) cell[c * ncell + pl(f, 2 * g, l, j, k)] = x.value[c];
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+      const size_t *fe = G.face[d].extent;
+      double *fd = face + d * 7 * nface;
+      for (int l = 0; l < g; ++l) {
+        const size_t i = outer + (d == 0) + l;
+        for (size_t j = 0; j < fe[1]; ++j)
+          for (size_t k = 0; k < fe[2]; ++k) {
+            const size_t idx = (i * fe[1] + j) * fe[2] + k;
+            const gamera_no_face_geometry &fg = G.face[d].value[idx];
+            const long long q = pl(f, g, l, (int)j, (int)k);
+            for (int c = 0; c < 3; ++c) {
+              fd[c * nface + q] = fg.centroid.value[c];
+              fd[(3 + c) * nface + q] = fg.area_vector.value[c];
+            }
+            fd[6 * nface + q] = b->background[f].face_flux[d][idx];
+          }
+      }
+      const size_t *ee = G.edge[d].extent;
+      const size_t *ve = G.vertex_extent;
+      double *ed = edge + d * 7 * nedge;
+      for (int l = 0; l < 5; ++l) {
+        const size_t i = l == 0 ? (size_t)g : (size_t)(outer - 3 + (l - 1));
+        if (i >= ee[0]) continue;
+        for (size_t j = 0; j < ee[1]; ++j)
+          for (size_t k = 0; k < ee[2]; ++k) {
+            const size_t idx = (i * ee[1] + j) * ee[2] + k;
+            const long long q = pl(f, 5, l, (int)j, (int)k);
+            hv[d * nedge + q] = G.edge[d].valid[idx];
+            const gamera_no_edge_geometry &eg = G.edge[d].value[idx];
+            size_t up[3] = {i, j, k};
+            ++up[d];
+            const gamera_no_vec3 &a = G.vertex[(i * ve[1] + j) * ve[2] + k];
+            const gamera_no_vec3 &z = G.vertex[(up[0] * ve[1] + up[1]) * ve[2] + up[2]];
+            for (int c = 0; c < 3; ++c) {
+              ed[c * nedge + q] = 0.5 * (a.value[c] + z.value[c]);
+              ed[(3 + c) * nedge + q] = eg.normal.value[c];
+            }
+            ed[6 * nedge + q] = eg.length;
+          }
+      }
+    }
+  }
+  e->pool_bytes = doubles * sizeof(double) + hv.size();
+  if (cudaMalloc(&e->pool, e->pool_bytes) != cudaSuccess ||
+      cudaMemcpy(e->pool, h.data(), doubles * sizeof(double), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy((char *)e->pool + doubles * sizeof(double), hv.data(), hv.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    gcs_earth_destroy(e);
+    gcs::set_api_error("cannot upload the Earth boundary geometry");
+    return -1;
+  }
+  const double *dp = (const double *)e->pool;
+  const unsigned char *vp = (const unsigned char *)e->pool + doubles * sizeof(double);
+  gcs::EarthDev &E = e->dev;
+  for (int c = 0; c < 3; ++c) E.cell_cen[c] = dp + c * ncell;
+  const double *fp = dp + 3 * ncell;
+  const double *ep = fp + 3 * 7 * nface;
+  for (int d = 0; d < 3; ++d) {
+    for (int c = 0; c < 3; ++c) {
+      E.face_cen[d][c] = fp + (d * 7 + c) * nface;
+      E.face_av[d][c] = fp + (d * 7 + 3 + c) * nface;
+      E.edge_mid[d][c] = ep + (d * 7 + c) * nedge;
+      E.edge_nrm[d][c] = ep + (d * 7 + 3 + c) * nedge;
+    }
+    E.face_bg[d] = fp + (d * 7 + 6) * nface;
+    E.edge_len[d] = ep + (d * 7 + 6) * nedge;
+    E.edge_valid[d] = vp + d * nedge;
+  }
+  E.gamma = b->startup->gamma;
+  E.rho_floor = b->density_floor;
+  E.p_floor = b->pressure_floor;
+  E.cfl = b->cfl;
+  E.strict_wall = b->strict_inner_gas_wall;
+  if (upload_wind(e, b->wind) != 0) {
+    gcs_earth_destroy(e);
+    return -1;
+  }
+  *out = e;
+  return 0;
+}
+
+int gcs_earth_set_wind(gcs_earth *earth, const gamera_solar_wind_series *wind) {
+  if (!earth) return -1;
+  if (cudaStreamSynchronize(earth->ctx->c.stream) != cudaSuccess) return -1;
+  return upload_wind(earth, wind);
+}
+
+void gcs_earth_destroy(gcs_earth *earth) {
+  if (!earth) return;
+  if (earth->ctx) cudaStreamSynchronize(earth->ctx->c.stream);
+  if (earth->pool) cudaFree(earth->pool);
+  if (earth->wind_pool) cudaFree(earth->wind_pool);
+  delete earth;
+}
+
+size_t gcs_earth_device_bytes(const gcs_earth *earth) {
+  return earth ? earth->pool_bytes + 9 * sizeof(double) * (size_t)earth->dev.wind.count : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,61 @@
+// Device form of the reference's Earth radial boundary callbacks
+// (cubedsphere/cubedsphere_earth_boundary.c) for the no-MI wall: radial
+// ghost states at both shells, the inner mass/energy flux trap and the
+// wind-driven outer / zero inner tangential EMF, as kernels run at the
+// reference step's callback positions (gcs_earth.cu).
+#pragma once
+
+#include "gcs_kernels.cuh"
+
+namespace gcs {
+
+// Monitor time series of the solar wind (nonorthogonal/src/solar_wind.h),
+// states as 8 doubles: density, pressure, velocity[3], magnetic[3].
+struct WindDev {
+  int count;
+  int linear;
+  const double *time;
+  const double *state;
+  double reference[3];
+  double time_offset, by, bz;
+};
+
+// Geometry of the radial boundary layers on the node plane of a face
+// (N1 x N2 per layer, six faces):
+//   cells: 2g layers, i = l (inner, l < g) or outer + l - g;
+//   outer ghost faces of family d: g layers, i = outer + (d == 0) + l;
+//   edges of family d: 5 layers, i = g (l = 0) or outer - 3 + (l - 1).
+struct EarthDev {
+  const double *cell_cen[3];
+  const double *face_cen[3][3], *face_av[3][3], *face_bg[3];
+  const double *edge_mid[3][3], *edge_nrm[3][3], *edge_len[3];
+  const unsigned char *edge_valid[3];
+  WindDev wind;
+  double gamma, rho_floor, p_floor, cfl;
+  int strict_wall;
+};
+
+// Times of one step with the device Earth boundary: the radial fill at
+// (current, previous) time, the EMF at step_time + step_dt / 2.
+struct EarthStep {
+  const EarthDev *dev;
+  double current_time, previous_time, step_time, step_dt;
+};
+
+void launch_earth_radial(const Ctx &X, const EarthDev &E, double current_time,
+                         double previous_time, cudaStream_t s);
+void launch_earth_trap(const Ctx &X, cudaStream_t s);
+void launch_earth_emf(const Ctx &X, const EarthDev &E, double step_time, double step_dt,
+                      cudaStream_t s);
+
+}  // namespace gcs
+
+// The C handle (gamera_cs_b200.h): device arrays of one context's boundary.
+struct gcs_context;
+struct gcs_earth {
+  gcs_context *ctx = nullptr;
+  gcs::EarthDev dev{};
+  void *pool = nullptr;          // geometry of the boundary layers
+  void *wind_pool = nullptr;     // monitor time series
+  size_t pool_bytes = 0;
+};

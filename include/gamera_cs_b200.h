@@ -379,6 +379,36 @@ int gcs_context_precision(const gcs_context *ctx);
 int gcs_context_set_bulk_threshold(gcs_context *ctx, double b0_threshold);
 int gcs_context_bulk_split(const gcs_context *ctx);
 
+/* Device Earth radial boundary (no-MI wall) of a context made from a host
+ * grid: the reference callbacks gamera_cs_earth_fill_radial_ghosts
+ * (radial ghost cells and faces of the state and old state at both shells,
+ * cell B recovered, cubedsphere_earth_boundary.c:27-212),
+ * gamera_cs_earth_inner_fluid_flux (:259-266) and gamera_cs_earth_no_mi_emf
+ * (:298-451) as kernels at the reference step's callback positions.
+ * gcs_earth_create copies the boundary layers' geometry from `grid`, the
+ * outer faces' B0 flux from boundary->background and the monitor series
+ * boundary->wind to the device; an MI-coupled wall (boundary->mi ready)
+ * is refused: it stays on the host callback path. */
+typedef struct gcs_earth gcs_earth;
+int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                     const gamera_cs_earth_boundary *boundary, gcs_earth **earth);
+/* Replace the monitor time series (e.g. a longer one). */
+int gcs_earth_set_wind(gcs_earth *earth, const gamera_solar_wind_series *wind);
+void gcs_earth_destroy(gcs_earth *earth);
+size_t gcs_earth_device_bytes(const gcs_earth *earth);
+/* One step on the device-resident state with the device Earth boundary:
+ * gamera_cs_advance_six_with_background_planned(..., radial_boundary =
+ * gamera_cs_earth_fill_radial_ghosts, current_time, previous_time,
+ * boundary) with options->fluid_flux_sync = gamera_cs_earth_inner_fluid_flux
+ * and options->edge_emf_sync = gamera_cs_earth_no_mi_emf, the boundary's
+ * step_time = current_time and step_dt = dt as the reference driver sets
+ * them (test_cubedsphere_dipole_background.c:667-668).  Callbacks in
+ * `options` are not called. */
+int gcs_context_step_earth(gcs_context *ctx, gcs_earth *earth,
+                           const gamera_no_advance_options *options,
+                           double predictor_ratio, double dt, double current_time,
+                           double previous_time);
+
 /* Upstream solar wind of a wind run (no reference counterpart; the
  * reference driver fixes it at n = 5 cm^-3, V = -400 km/s, T = 1e5 K,
  * Bz = -5 nT, test_cubedsphere_dipole_background.c:282-294): density

@@ -326,6 +326,52 @@ typedef struct {
   const double *potential_v[2];
 } gamera_cs_mi_analysis_view;
 
+/* nonorthogonal/src/solar_wind.h:10-15 */
+enum {
+  GAMERA_WIND_X = 0,
+  GAMERA_WIND_Y = 1,
+  GAMERA_WIND_Z = 2,
+  GAMERA_WIND_DIM = 3
+};
+
+/* nonorthogonal/src/solar_wind.h:17-22 */
+typedef struct {
+  double density;
+  double pressure;
+  double velocity[GAMERA_WIND_DIM];
+  double magnetic[GAMERA_WIND_DIM];
+} gamera_solar_wind_state;
+
+/* nonorthogonal/src/solar_wind.h:24-35 */
+typedef struct {
+  size_t count;
+  double *time;
+  gamera_solar_wind_state *state;
+  double reference[GAMERA_WIND_DIM];
+  double time_offset;
+  double by_coefficient;
+  double bz_coefficient;
+  double bx_offset;
+  int enforce_bx_relation;
+  int linear_interpolation;
+} gamera_solar_wind_series;
+
+struct gamera_cs_mi_dipole;
+
+/* cubedsphere/cubedsphere_earth_boundary.h:13-24 */
+typedef struct {
+  const gamera_cs_earth_startup *startup;
+  const gamera_solar_wind_series *wind;
+  const gamera_no_background_field *background; /* six faces */
+  const struct gamera_cs_mi_dipole *mi;          /* NULL: no-MI wall */
+  double density_floor;
+  double pressure_floor;
+  double step_time;
+  double step_dt;
+  double cfl;
+  int strict_inner_gas_wall;
+} gamera_cs_earth_boundary;
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,155 @@
+"""GPU parity of the device Earth radial boundary (no-MI wall).
+
+The same reference-built wind case (grid, state, dipole background) is
+advanced twice from identical inputs:
+  * by the compiled reference's own step with its own callbacks
+    gamera_cs_earth_fill_radial_ghosts / gamera_cs_earth_inner_fluid_flux /
+    gamera_cs_earth_no_mi_emf (oracle/_ref), on the CPU;
+  * by gcs_context_step_earth, the step with those callbacks as kernels.
+The monitor series has three samples with linear interpolation, a tilted
+planar front (By/Bz coefficients) and a time offset, so the ballistic
+mapping, interpolation and upstream-to-tail weights all enter.  Tolerance:
+1e-12 normwise per array per step (device libm may differ from the host's
+in the last bit of sqrt/acos/exp), growing by 10x per chained step as the
+plain step parity test allows.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gamera_cube_b200 import abi
+from oracle import refbind
+from tests.parity_util import compare_state
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["conserved", "old_conserved", "cell_magnetic", "old_cell_magnetic"] + \
+        ["face_flux%d" % d for d in range(3)] + ["old_face_flux%d" % d for d in range(3)]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import gamera_cube_b200
+    return gamera_cube_b200.lib
+
+
+def wind_series(keep):
+    times = np.array([0.0, 0.004, 0.012])
+    states = (abi.SolarWindState * 3)()
+    for q, (rho, vx, by, bz) in enumerate([(5.0, -4.0, 0.05, -0.08),
+                                           (7.5, -4.6, -0.02, 0.10),
+                                           (4.0, -3.5, 0.03, -0.12)]):
+        states[q].density = rho
+        states[q].pressure = 0.6 * rho / 5.0
+        states[q].velocity[:] = [vx, 0.2, -0.1]
+        states[q].magnetic[:] = [0.02, by, bz]
+    t = (C.c_double * 3)(*times)
+    keep += [t, states]
+    w = abi.SolarWindSeries()
+    w.count = 3
+    w.time = t
+    w.state = states
+    w.reference[:] = [28.0, 0.0, 0.0]
+    w.time_offset = 0.001
+    w.by_coefficient = 0.2
+    w.bz_coefficient = -0.1
+    w.linear_interpolation = 1
+    return w
+
+
+def boundary(startup, wind, background, strict):
+    b = abi.EarthBoundary()
+    b.startup = C.pointer(startup)
+    b.wind = C.pointer(wind)
+    b.background = background
+    b.mi = None
+    b.density_floor = 1e-6
+    b.pressure_floor = 1e-8
+    b.cfl = 0.3
+    b.strict_inner_gas_wall = strict
+    return b
+
+
+@pytest.mark.parametrize("strict", [0, 1])
+def test_earth_boundary_matches_reference(lib, strict):
+    if not refbind.ref_available():
+        pytest.skip("reference library not built")
+    R = refbind.ref()
+    ref = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    gpu = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    keep = []
+    startup = abi.EarthStartup()
+    startup.gamma = 5.0 / 3.0
+    wind = wind_series(keep)
+    b_ref = boundary(startup, wind, ref.background, strict)
+    b_gpu = boundary(startup, wind, gpu.background, strict)
+
+    ropts = abi.AdvanceOptions.from_buffer_copy(ref.options.contents)
+    ropts.fluid_flux_sync = C.cast(R.gamera_cs_earth_inner_fluid_flux, C.c_void_p).value
+    ropts.edge_emf_sync = C.cast(R.gamera_cs_earth_no_mi_emf, C.c_void_p).value
+    ropts.edge_emf_context = C.cast(C.pointer(b_ref), C.c_void_p).value
+    radial = C.cast(R.gamera_cs_earth_fill_radial_ghosts, C.c_void_p).value
+    gopts = abi.AdvanceOptions.from_buffer_copy(gpu.options.contents)
+
+    ctx = lib.gcs_context_create(gpu.grid, gpu.active, gpu.ghost)
+    assert ctx, lib.gcs_last_error()
+    earth = C.c_void_p()
+    try:
+        assert lib.gcs_context_upload_background(ctx, gpu.background) == 0
+        assert lib.gcs_context_upload_state(ctx, gpu.storage) == 0
+        assert lib.gcs_earth_create(ctx, gpu.grid, C.byref(b_gpu), C.byref(earth)) == 0, \
+            lib.gcs_last_error()
+        assert lib.gcs_earth_device_bytes(earth) > 0
+        time, dt_prev = 0.0, 0.0
+        for s in range(3):
+            local = ref.local_timestep()
+            dt = 0.5 * local if dt_prev == 0.0 else min(0.5 * local, 1.25 * dt_prev)
+            ratio = 0.0 if dt_prev == 0.0 else 0.5 * dt / dt_prev
+            prev = time if s == 0 else time - dt_prev
+            b_ref.step_time, b_ref.step_dt = time, dt
+            assert R.gamera_cs_advance_six_with_background_planned(
+                ref.grid, ref.storage, ref.active, ref.ghost, ratio, dt, C.byref(ropts),
+                ref.background, R.fx_plan(ref.handle), radial, time, prev,
+                C.cast(C.pointer(b_ref), C.c_void_p)) == 0
+            assert lib.gcs_context_step_earth(ctx, earth, C.byref(gopts), ratio, dt, time,
+                                              prev) == 0, lib.gcs_context_error(ctx)
+            assert lib.gcs_context_download_state(ctx, gpu.storage, 0) == 0
+            res = compare_state(gpu, ref, NAMES)
+            bad = {k: v for k, v in res.items() if not v[0] <= 1e-12 * 10 ** s}
+            assert not bad, "step %d: %s" % (s, bad)
+            time += dt
+            dt_prev = dt
+        # the boundary acted: inner ghosts mirror, outer ghosts follow the wind
+        u = ref.arrays(0)["conserved"]
+        assert not np.allclose(u[0], u[4]) or not np.allclose(u[-1], u[-5])
+    finally:
+        if earth:
+            lib.gcs_earth_destroy(earth)
+        lib.gcs_context_destroy(ctx)
+        ref.close()
+        gpu.close()
+
+
+def test_earth_boundary_rejects_bad_input(lib):
+    if not refbind.ref_available():
+        pytest.skip("reference library not built")
+    case = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    ctx = lib.gcs_context_create(case.grid, case.active, case.ghost)
+    assert ctx
+    try:
+        keep = []
+        startup = abi.EarthStartup()
+        startup.gamma = 5.0 / 3.0
+        wind = wind_series(keep)
+        b = boundary(startup, wind, case.background, 0)
+        b.density_floor = 0.0
+        earth = C.c_void_p()
+        assert lib.gcs_earth_create(ctx, case.grid, C.byref(b), C.byref(earth)) == -1
+        b.density_floor = 1e-6
+        wind.count = 0
+        assert lib.gcs_earth_create(ctx, case.grid, C.byref(b), C.byref(earth)) == -1
+        assert not earth
+    finally:
+        lib.gcs_context_destroy(ctx)
+        case.close()

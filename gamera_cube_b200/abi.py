@@ -258,7 +258,7 @@ class EnsembleConfig(C.Structure):
 
 def ensemble_signatures():
     P = C.POINTER
-    return {
+    sig = {
         "gcs_context_create_wind": (C.c_void_p, [C.c_size_t, C.c_size_t, C.c_ulonglong,
                                                  P(WindDriver)]),
         "gcs_tile_limit": (C.c_int, [C.c_int]),
@@ -289,6 +289,27 @@ def ensemble_signatures():
         "gcs_context_step_earth": (C.c_int, [C.c_void_p, C.c_void_p, P(AdvanceOptions),
                                              C.c_double, C.c_double, C.c_double,
                                              C.c_double]),
+    }
+    sig.update(earth_callback_signatures())
+    return sig
+
+
+def earth_callback_signatures():
+    """The reference's Earth radial-boundary callbacks (same in the reference
+    library and in this one)."""
+    P = C.POINTER
+    c_sz3 = C.c_size_t * 3
+    return {
+        "gamera_cs_earth_fill_radial_ghosts": (
+            C.c_int, [P(Grid), P(Storage), c_sz3, C.c_size_t, C.c_double, C.c_double,
+                      C.c_void_p]),
+        "gamera_cs_earth_fill_radial_ghosts_face": (
+            C.c_int, [P(Grid), P(Storage), c_sz3, C.c_size_t, C.c_double, C.c_double,
+                      C.c_void_p, C.c_int]),
+        "gamera_cs_earth_inner_fluid_flux": (
+            C.c_int, [P(Storage), P(Grid), c_sz3, c_sz3, C.c_void_p]),
+        "gamera_cs_earth_no_mi_emf": (
+            C.c_int, [P(Storage), P(Grid), c_sz3, c_sz3, C.c_void_p]),
     }
 
 

@@ -391,9 +391,29 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
                       C.stream) != cudaSuccess)
     return -1;
   C.reset_status_async();
-  Hooks hk{grid, storage, active, ghost, radial, t, tprev, radial_ctx, options};
-  const bool hooks = radial || options->fluid_flux_sync || options->edge_emf_sync;
-  int rc = run_step(ctx, O, 0, hooks ? &hk : nullptr);
+  // The reference's Earth callbacks of this library run as device kernels
+  // inside the step (no host round trip) unless the MI coupling is ready.
+  const gamera_cs_earth_boundary *eb = nullptr;
+  if (grid != nullptr && radial == gamera_cs_earth_fill_radial_ghosts &&
+      options->fluid_flux_sync == gamera_cs_earth_inner_fluid_flux &&
+      options->edge_emf_sync == gamera_cs_earth_no_mi_emf &&
+      options->edge_emf_context == radial_ctx && radial_ctx != nullptr) {
+    eb = (const gamera_cs_earth_boundary *)radial_ctx;
+    if (eb->mi != nullptr && gamera_cs_mi_dipole_ready(eb->mi)) eb = nullptr;
+  }
+  int rc;
+  if (eb != nullptr) {
+    // the reference's EMF callback fails on these (cubedsphere_earth_boundary.c:388-389)
+    if (!std::isfinite(eb->step_time) || !(eb->step_dt > 0.0)) return -1;
+    gcs_earth *earth = gcs::earth_for(C, grid, eb, false);
+    if (earth == nullptr) return -1;
+    const gcs::EarthStep es{&earth->dev, t, tprev, eb->step_time, eb->step_dt};
+    rc = run_step(ctx, O, 0, nullptr, &es);
+  } else {
+    Hooks hk{grid, storage, active, ghost, radial, t, tprev, radial_ctx, options};
+    const bool hooks = radial || options->fluid_flux_sync || options->edge_emf_sync;
+    rc = run_step(ctx, O, 0, hooks ? &hk : nullptr);
+  }
   const bool fail = device_failed(C);
   if (fail) report_failure(C);
   // Emergency-diffusion statistics accumulate in the caller's storage.
@@ -903,6 +923,7 @@ int gcs_context_dims(const gcs_context *ctx, size_t active[3], size_t *ghost) {
 
 void gcs_context_destroy(gcs_context *ctx) {
   if (!ctx) return;
+  gcs::earth_forget(ctx->c);
   for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   delete ctx;
 }
@@ -955,7 +976,7 @@ int gcs_context_step_earth(gcs_context *ctx, gcs_earth *earth,
                            const gamera_no_advance_options *options,
                            double ratio, double dt, double current_time,
                            double previous_time) {
-  if (!ctx || !earth || earth->ctx != ctx || !options) return -1;
+  if (!ctx || !earth || earth->C != &ctx->c || !options) return -1;
   if (!std::isfinite(current_time) || !std::isfinite(previous_time) || !(dt > 0.0) ||
       !std::isfinite(dt)) {
     set_last("invalid step times");

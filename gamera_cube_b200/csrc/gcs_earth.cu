@@ -15,7 +15,10 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "gcs_kernel_util.cuh"
@@ -28,7 +31,7 @@ struct WindState {
   double rho, p, v[3], b[3];
 };
 
-__device__ inline WindState wind_load(const WindDev &w, int q) {
+__host__ __device__ inline WindState wind_load(const WindDev &w, int q) {
   const double *a = w.state + 8LL * q;
   WindState s;
   s.rho = a[0];
@@ -41,7 +44,7 @@ __device__ inline WindState wind_load(const WindDev &w, int q) {
 }
 
 // solar_wind.c:8-22
-__device__ inline bool wind_finite(const WindState &s) {
+__host__ __device__ inline bool wind_finite(const WindState &s) {
   if (!isfinite(s.rho) || !isfinite(s.p) || s.rho <= 0.0 || s.p <= 0.0) return false;
   for (int c = 0; c < 3; ++c)
     if (!isfinite(s.v[c]) || !isfinite(s.b[c])) return false;
@@ -49,7 +52,7 @@ __device__ inline bool wind_finite(const WindState &s) {
 }
 
 // solar_wind.c:134-160 (binary search of :104-117, interpolation :119-132)
-__device__ bool wind_sample_time(const WindDev &w, double time, WindState *out) {
+__host__ __device__ bool wind_sample_time(const WindDev &w, double time, WindState *out) {
   if (!isfinite(time)) return false;
   if (w.count == 1 || time <= w.time[0]) {
     *out = wind_load(w, 0);
@@ -84,7 +87,7 @@ __device__ bool wind_sample_time(const WindDev &w, double time, WindState *out) 
 }
 
 // Planar-front ballistic mapping, solar_wind.c:162-200.
-__device__ bool wind_sample_at(const WindDev &w, const double x[3], double t,
+__host__ __device__ bool wind_sample_at(const WindDev &w, const double x[3], double t,
                                WindState *out) {
   if (!isfinite(t)) return false;
   const double monitor = t + w.time_offset;
@@ -106,7 +109,7 @@ __device__ bool wind_sample_at(const WindDev &w, const double x[3], double t,
 
 // Upstream-to-tail weight, solar_wind.c:202-225, on the state the mapping
 // returns for the same point and time.
-__device__ bool wind_weight(const double x[3], const WindState &s, double *weight) {
+__host__ __device__ bool wind_weight(const double x[3], const WindState &s, double *weight) {
   double r2 = 0.0, v2 = 0.0, cosine = 0.0;
   for (int c = 0; c < 3; ++c) {
     r2 += x[c] * x[c];
@@ -130,7 +133,7 @@ __device__ bool wind_weight(const double x[3], const WindState &s, double *weigh
 }
 
 // cubedsphere_earth_boundary.c:16-25
-__device__ inline bool sample_wind(const WindDev &w, const double x[3], double t,
+__host__ __device__ inline bool sample_wind(const WindDev &w, const double x[3], double t,
                                    WindState *s, double *weight) {
   return wind_sample_at(w, x, t, s) && wind_weight(x, *s, weight);
 }
@@ -501,26 +504,22 @@ int upload_wind(gcs_earth *e, const gamera_solar_wind_series *w) {
   return 0;
 }
 
-}  // namespace
-
-extern "C" {
-
-int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
-                     const gamera_cs_earth_boundary *b, gcs_earth **out) {
-  if (!out) return -1;
+int earth_create(gcs::Context &C, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                 const gamera_cs_earth_boundary *b, gcs_earth **out,
+                 bool allow_mi = false) {
   *out = nullptr;
-  if (!ctx || !grid || !b || !b->startup || !b->wind || !b->background ||
+  if (!grid || !b || !b->startup || !b->wind || !b->background ||
       !std::isfinite(b->density_floor) || !(b->density_floor > 0.0) ||
       !std::isfinite(b->pressure_floor) || !(b->pressure_floor > 0.0) ||
       !(b->cfl > 0.0) || !std::isfinite(b->startup->gamma)) {
     gcs::set_api_error("invalid Earth boundary");
     return -1;
   }
-  if (b->mi != nullptr && gamera_cs_mi_dipole_ready(b->mi)) {
+  if (!allow_mi && b->mi != nullptr && gamera_cs_mi_dipole_ready(b->mi)) {
     gcs::set_api_error("the MI-coupled inner wall needs the host callback path");
     return -1;
   }
-  const gcs::Dims &D = ctx->c.X.D;
+  const gcs::Dims &D = C.X.D;
   for (int f = 0; f < gcs::kFaces; ++f) {
     const gamera_no_grid &g = grid[f];
     if ((int)g.cell_extent[0] != D.E0 || (int)g.cell_extent[1] != D.E1 ||
@@ -538,7 +537,7 @@ int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_
   }
   gcs_earth *e = new (std::nothrow) gcs_earth;
   if (!e) return -1;
-  e->ctx = ctx;
+  e->C = &C;
   const long long P = (long long)D.N1 * D.N2;
   const int g = D.g, outer = D.g + D.nr;
   const long long ncell = 6LL * 2 * g * P, nface = 6LL * g * P, nedge = 6LL * 5 * P;
@@ -643,15 +642,356 @@ int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_
   return 0;
 }
 
+gcs::WindDev host_wind(const gamera_solar_wind_series *w) {
+  gcs::WindDev W{};
+  W.count = (int)w->count;
+  W.linear = w->linear_interpolation;
+  W.time = w->time;
+  W.state = (const double *)w->state;
+  for (int c = 0; c < 3; ++c) W.reference[c] = w->reference[c];
+  W.time_offset = w->time_offset;
+  W.by = w->by_coefficient;
+  W.bz = w->bz_coefficient;
+  return W;
+}
+
+// cubedsphere_earth_boundary.c:9-14, plus a usable series
+bool boundary_ok(const gamera_cs_earth_boundary *b) {
+  return b != nullptr && b->startup != nullptr && b->wind != nullptr &&
+         b->background != nullptr && std::isfinite(b->density_floor) &&
+         b->density_floor > 0.0 && std::isfinite(b->pressure_floor) &&
+         b->pressure_floor > 0.0 && b->wind->count >= 1 && b->wind->time != nullptr &&
+         b->wind->state != nullptr;
+}
+
+// Cache of device boundaries per (context, boundary).
+struct EarthEntry {
+  gcs_earth *earth;
+  const gamera_no_background_field *background;
+  std::vector<double> time;
+  std::vector<gamera_solar_wind_state> state;
+};
+std::mutex g_earth_mutex;
+std::map<std::pair<const gcs::Context *, const void *>, EarthEntry> g_earth;
+
+bool same_series(const EarthEntry &e, const gamera_solar_wind_series *w) {
+  return e.time.size() == w->count &&
+         std::memcmp(e.time.data(), w->time, w->count * sizeof(double)) == 0 &&
+         std::memcmp(e.state.data(), w->state, w->count * sizeof(gamera_solar_wind_state)) == 0;
+}
+
+void remember_series(EarthEntry &e, const gamera_solar_wind_series *w) {
+  e.time.assign(w->time, w->time + w->count);
+  e.state.assign(w->state, w->state + w->count);
+}
+
+}  // namespace
+
+namespace gcs {
+
+gcs_earth *earth_for(Context &C, const gamera_no_grid grid[kFaces],
+                     const gamera_cs_earth_boundary *b, bool allow_mi) {
+  if (!boundary_ok(b) || !(b->cfl > 0.0)) {
+    set_api_error("invalid Earth boundary");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_earth_mutex);
+  const auto key = std::make_pair((const Context *)&C, (const void *)b);
+  auto it = g_earth.find(key);
+  if (it != g_earth.end() && it->second.background != b->background) {
+    gcs_earth_destroy(it->second.earth);
+    g_earth.erase(it);
+    it = g_earth.end();
+  }
+  if (it == g_earth.end()) {
+    gcs_earth *e = nullptr;
+    if (earth_create(C, grid, b, &e, allow_mi) != 0) return nullptr;
+    EarthEntry en{e, b->background, {}, {}};
+    remember_series(en, b->wind);
+    it = g_earth.emplace(key, std::move(en)).first;
+  } else if (!same_series(it->second, b->wind)) {
+    if (cudaStreamSynchronize(C.stream) != cudaSuccess ||
+        upload_wind(it->second.earth, b->wind) != 0)
+      return nullptr;
+    remember_series(it->second, b->wind);
+  }
+  // floors, CFL, wall flag and the front mapping may change between calls
+  EarthDev &E = it->second.earth->dev;
+  const WindDev W = host_wind(b->wind);
+  E.wind.linear = W.linear;
+  for (int c = 0; c < 3; ++c) E.wind.reference[c] = W.reference[c];
+  E.wind.time_offset = W.time_offset;
+  E.wind.by = W.by;
+  E.wind.bz = W.bz;
+  E.gamma = b->startup->gamma;
+  E.rho_floor = b->density_floor;
+  E.p_floor = b->pressure_floor;
+  E.cfl = b->cfl;
+  E.strict_wall = b->strict_inner_gas_wall;
+  return it->second.earth;
+}
+
+void earth_forget(const Context &C) {
+  std::lock_guard<std::mutex> lock(g_earth_mutex);
+  for (auto it = g_earth.begin(); it != g_earth.end();) {
+    if (it->first.first == &C) {
+      gcs_earth_destroy(it->second.earth);
+      it = g_earth.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+}  // namespace gcs
+
+namespace {
+
+// Inner ghost cells of one face with the MI drift velocity
+// (cubedsphere_earth_boundary.c:55-69), on host storage.
+int mi_inner_cells(const gamera_no_grid &grid, gamera_no_storage &st, size_t ghost,
+                   const gamera_cs_earth_boundary *b) {
+  const size_t *ex = grid.cell_extent;
+  for (int old = 0; old < 2; ++old) {
+    double *u = old ? st.old_conserved : st.conserved;
+    for (size_t i = 0; i < ghost; ++i)
+      for (size_t j = 0; j < ex[1]; ++j)
+        for (size_t k = 0; k < ex[2]; ++k) {
+          const size_t t = (i * ex[1] + j) * ex[2] + k;
+          const size_t s = ((2 * ghost - 1 - i) * ex[1] + j) * ex[2] + k;
+          gcs::Prim p;
+          if (gcs::cons_to_prim(&u[s * 5], b->startup->gamma, b->density_floor,
+                                b->pressure_floor, &p))
+            return -1;
+          const gamera_no_vec3 x = grid.cell[t].centroid;
+          const double radius = sqrt(x.value[0] * x.value[0] + x.value[1] * x.value[1] +
+                                     x.value[2] * x.value[2]);
+          if (!(radius > 0.0)) return -1;
+          const gamera_no_vec3 v = {{p.vx, p.vy, p.vz}};
+          gamera_no_vec3 gv;
+          if (gamera_cs_mi_dipole_ghost_velocity(b->mi, x, v, &gv) != 0) return -1;
+          if (b->strict_inner_gas_wall)
+            for (int c = 0; c < 3; ++c) gv.value[c] = 0.5 * (gv.value[c] + v.value[c]);
+          p.vx = gv.value[0];
+          p.vy = gv.value[1];
+          p.vz = gv.value[2];
+          if (gcs::prim_to_cons(p, b->startup->gamma, b->density_floor, b->pressure_floor,
+                                &u[t * 5]))
+            return -1;
+        }
+  }
+  return 0;
+}
+
+int fill_radial(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                gamera_no_storage storage[GAMERA_CS_FACE_COUNT], const size_t active[3],
+                size_t ghost, double t, double tprev, void *context, int receiver) {
+  const auto *b = (const gamera_cs_earth_boundary *)context;
+  if (!grid || !storage || !active || ghost < 4 || !boundary_ok(b) || !std::isfinite(t) ||
+      !std::isfinite(tprev))
+    return -1;
+  gcs::Context *C = gcs::context_for_grid(grid, active, ghost);
+  if (!C) return -1;
+  gcs_earth *e = gcs::earth_for(*C, grid, b, true);
+  if (!e || C->upload_state(storage) != 0) return -1;
+  C->reset_status_async();
+  gcs::launch_earth_radial(C->X, e->dev, t, tprev, C->stream);
+  gcs::DevStatus s;
+  if (cudaGetLastError() != cudaSuccess || C->read_status(&s) != 0 || s.first != 0) {
+    C->reset_status_async();
+    return -1;
+  }
+  for (int f = 0; f < gcs::kFaces; ++f) {
+    if (receiver >= 0 && f != receiver) continue;
+    gamera_no_storage &st = storage[f];
+    if (C->transfer_array(f, gcs::kArrU, 0, false, st.conserved) ||
+        C->transfer_array(f, gcs::kArrUo, 0, false, st.old_conserved) ||
+        C->transfer_array(f, gcs::kArrB, 0, false, (double *)st.cell_magnetic) ||
+        C->transfer_array(f, gcs::kArrBo, 0, false, (double *)st.old_cell_magnetic))
+      return -1;
+    for (int d = 0; d < 3; ++d)
+      if (C->transfer_array(f, gcs::kArrP, d, false, st.face_flux[d]) ||
+          C->transfer_array(f, gcs::kArrPo, d, false, st.old_face_flux[d]))
+        return -1;
+    if (b->mi && gamera_cs_mi_dipole_ready(b->mi) && mi_inner_cells(grid[f], st, ghost, b))
+      return -1;
+  }
+  return 0;
+}
+
+bool host_flux_density(const gamera_no_grid *grid, const double *flux, int d, size_t i,
+                       size_t j, size_t k, double *out) {
+  const size_t *fe = grid->face[d].extent;
+  if (!flux || i >= fe[0] || j >= fe[1] || k >= fe[2]) return false;
+  const size_t idx = (i * fe[1] + j) * fe[2] + k;
+  const double area = grid->face[d].value[idx].area;
+  if (!(area > 0.0)) return false;
+  *out = flux[idx] / area;
+  return std::isfinite(*out);
+}
+
+void edge_mid(const gamera_no_grid *grid, int d, size_t i, size_t j, size_t k, double x[3]) {
+  size_t up[3] = {i, j, k};
+  ++up[d];
+  const size_t *ve = grid->vertex_extent;
+  const gamera_no_vec3 &a = grid->vertex[(i * ve[1] + j) * ve[2] + k];
+  const gamera_no_vec3 &z = grid->vertex[(up[0] * ve[1] + up[1]) * ve[2] + up[2]];
+  for (int c = 0; c < 3; ++c) x[c] = 0.5 * (a.value[c] + z.value[c]);
+}
+
+}  // namespace
+
+extern "C" {
+
+/* cubedsphere_earth_boundary.c:212-231.  Runs the device kernels of the
+ * drop-in step on the grid's context (state uploaded, ghosts downloaded);
+ * a ready MI coupling sets the inner ghost velocities on the host. */
+int gamera_cs_earth_fill_radial_ghosts(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                       gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                       const size_t active[3], size_t ghost,
+                                       double current_time, double previous_time,
+                                       void *context) {
+  return fill_radial(grid, storage, active, ghost, current_time, previous_time, context, -1);
+}
+
+int gamera_cs_earth_fill_radial_ghosts_face(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                            gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                            const size_t active[3], size_t ghost,
+                                            double current_time, double previous_time,
+                                            void *context, int face) {
+  if (face < 0 || face >= GAMERA_CS_FACE_COUNT) return -1;
+  return fill_radial(grid, storage, active, ghost, current_time, previous_time, context,
+                     face);
+}
+
+/* cubedsphere_earth_boundary.c:259-266 with nonorthogonal_step.c:35-72,
+ * on one face's host storage. */
+int gamera_cs_earth_inner_fluid_flux(gamera_no_storage *storage, const gamera_no_grid *grid,
+                                     const size_t lower[3], const size_t upper[3],
+                                     void *context) {
+  (void)grid;
+  (void)context;
+  if (!storage || !lower || !upper || !storage->fluid_face_flux[0]) return -1;
+  const size_t *fe = storage->face_extent[0];
+  if (lower[0] >= fe[0] || lower[1] >= upper[1] || lower[2] >= upper[2] ||
+      upper[1] > fe[1] || upper[2] > fe[2])
+    return -1;
+  for (size_t j = lower[1]; j < upper[1]; ++j)
+    for (size_t k = lower[2]; k < upper[2]; ++k) {
+      double *fl = &storage->fluid_face_flux[0][((lower[0] * fe[1] + j) * fe[2] + k) * 5];
+      if (fl[0] > 0.0) {
+        fl[0] = 0.0;
+        if (fl[4] > 0.0) fl[4] = 0.0;
+      }
+    }
+  return 0;
+}
+
+/* cubedsphere_earth_boundary.c:381-451 on one face's host storage: the
+ * same arithmetic as the device EMF kernels. */
+int gamera_cs_earth_no_mi_emf(gamera_no_storage *storage, const gamera_no_grid *grid,
+                              const size_t lower[3], const size_t upper[3], void *context) {
+  const auto *b = (const gamera_cs_earth_boundary *)context;
+  if (!storage || !grid || !lower || !upper || !boundary_ok(b) ||
+      !std::isfinite(b->step_time) || !(b->step_dt > 0.0))
+    return -1;
+  const gcs::WindDev W = host_wind(b->wind);
+  const double tmid = b->step_time + 0.5 * b->step_dt;
+  const size_t outer = upper[0];
+  const size_t first = outer > 3 ? outer - 3 : 0;
+  for (int d = 0; d < 3; ++d) {
+    const size_t *ee = grid->edge[d].extent;
+    for (size_t i = first; i <= outer && i < ee[0]; ++i)
+      for (size_t j = 0; j < ee[1]; ++j)
+        for (size_t k = 0; k < ee[2]; ++k) {
+          const size_t idx = (i * ee[1] + j) * ee[2] + k;
+          if (!grid->edge[d].valid[idx]) continue;
+          double x[3];
+          edge_mid(grid, d, i, j, k, x);
+          gcs::WindState w;
+          double wt;
+          if (!gcs::sample_wind(W, x, tmid, &w, &wt)) return -1;
+          if (i < outer) wt /= 1.0 + (double)(outer - i);
+          const double el[3] = {-(w.v[1] * w.b[2] - w.v[2] * w.b[1]),
+                                -(w.v[2] * w.b[0] - w.v[0] * w.b[2]),
+                                -(w.v[0] * w.b[1] - w.v[1] * w.b[0])};
+          const gamera_no_edge_geometry &g = grid->edge[d].value[idx];
+          double li = 0.0;
+          for (int c = 0; c < 3; ++c) li += el[c] * g.normal.value[c] * g.length;
+          storage->edge_emf[d][idx] = (1.0 - wt) * storage->edge_emf[d][idx] + wt * li;
+        }
+  }
+  {
+    const size_t i = upper[0];
+    if (i == 0 || !(b->cfl > 0.0)) return -1;
+    const size_t *ej = grid->edge[1].extent, *ek = grid->edge[2].extent;
+    for (size_t j = lower[1]; j <= upper[1]; ++j)
+      for (size_t k = lower[2]; k <= upper[2]; ++k) {
+        if (j == 0 || k == 0 || i >= ej[0] || j >= ej[1] || k >= ej[2] || i >= ek[0] ||
+            j >= ek[1] || k >= ek[2])
+          continue;
+        const size_t ij = (i * ej[1] + j) * ej[2] + k, ik = (i * ek[1] + j) * ek[2] + k;
+        if (!grid->edge[1].valid[ij] || !grid->edge[2].valid[ik]) continue;
+        double bikp, bikm, bkip, bkim, bjip, bjim, bijp, bijm;
+        const double *const *pf = storage->predicted_face_flux;
+        if (!host_flux_density(grid, pf[0], 0, i, j, k, &bikp) ||
+            !host_flux_density(grid, pf[0], 0, i, j, k - 1, &bikm) ||
+            !host_flux_density(grid, pf[2], 2, i, j, k, &bkip) ||
+            !host_flux_density(grid, pf[2], 2, i - 1, j, k, &bkim) ||
+            !host_flux_density(grid, pf[1], 1, i, j, k, &bjip) ||
+            !host_flux_density(grid, pf[1], 1, i - 1, j, k, &bjim) ||
+            !host_flux_density(grid, pf[0], 0, i, j, k, &bijp) ||
+            !host_flux_density(grid, pf[0], 0, i, j - 1, k, &bijm))
+          return -1;
+        const double cur_j = (bikp - bikm) - (bkip - bkim);
+        const double cur_k = (bjip - bjim) - (bijp - bijm);
+        const double dl = sqrt(grid->edge[1].value[ij].length * grid->edge[2].value[ik].length);
+        double xj[3], xk[3];
+        edge_mid(grid, 1, i, j, k, xj);
+        edge_mid(grid, 2, i, j, k, xk);
+        gcs::WindState wj, wk;
+        double wtj, wtk;
+        if (!(dl > 0.0) || !gcs::sample_wind(W, xj, tmid, &wj, &wtj) ||
+            !gcs::sample_wind(W, xk, tmid, &wk, &wtk))
+          return -1;
+        const double csq = W.by * W.by + W.bz * W.bz;
+        const double front = fmax(fabs(wj.v[0]), fabs(wk.v[0])) / sqrt(1.0 + csq);
+        const double speed = fmin(front, b->cfl * dl / b->step_dt);
+        storage->edge_emf[1][ij] += wtj * speed * cur_j * dl;
+        storage->edge_emf[2][ik] += wtk * speed * cur_k * dl;
+      }
+  }
+  for (int d = 1; d <= 2; ++d) {
+    const size_t *ee = grid->edge[d].extent;
+    for (size_t j = 0; j < ee[1]; ++j)
+      for (size_t k = 0; k < ee[2]; ++k) {
+        const size_t idx = (lower[0] * ee[1] + j) * ee[2] + k;
+        if (grid->edge[d].valid[idx]) storage->edge_emf[d][idx] = 0.0;
+      }
+  }
+  if (b->mi && gamera_cs_mi_dipole_ready(b->mi) &&
+      gamera_cs_mi_dipole_apply_inner_emf(b->mi, storage, grid, lower[0]) != 0)
+    return -1;
+  return 0;
+}
+
+int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                     const gamera_cs_earth_boundary *b, gcs_earth **out) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (!ctx) return -1;
+  return earth_create(ctx->c, grid, b, out);
+}
+
 int gcs_earth_set_wind(gcs_earth *earth, const gamera_solar_wind_series *wind) {
   if (!earth) return -1;
-  if (cudaStreamSynchronize(earth->ctx->c.stream) != cudaSuccess) return -1;
+  if (cudaStreamSynchronize(earth->C->stream) != cudaSuccess) return -1;
   return upload_wind(earth, wind);
 }
 
 void gcs_earth_destroy(gcs_earth *earth) {
   if (!earth) return;
-  if (earth->ctx) cudaStreamSynchronize(earth->ctx->c.stream);
+  if (earth->C) cudaStreamSynchronize(earth->C->stream);
   if (earth->pool) cudaFree(earth->pool);
   if (earth->wind_pool) cudaFree(earth->wind_pool);
   delete earth;

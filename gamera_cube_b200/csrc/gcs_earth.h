@@ -6,6 +6,9 @@
 #pragma once
 
 #include "gcs_kernels.cuh"
+#include "gamera_cs_types.h"
+
+struct gcs_earth;
 
 namespace gcs {
 
@@ -48,12 +51,22 @@ void launch_earth_trap(const Ctx &X, cudaStream_t s);
 void launch_earth_emf(const Ctx &X, const EarthDev &E, double step_time, double step_dt,
                       cudaStream_t s);
 
+struct Context;
+// The device boundary the drop-in step and the host entry points use for
+// (context, boundary): created on first use, its wind series, floors, CFL
+// and wall flag refreshed from `b` on every call.  NULL on failure.
+// With allow_mi a ready MI coupling is accepted (the host entry points
+// then set the inner ghost velocities themselves).
+gcs_earth *earth_for(Context &C, const gamera_no_grid grid[kFaces],
+                     const gamera_cs_earth_boundary *b, bool allow_mi);
+// Drop the boundaries cached for a context being destroyed.
+void earth_forget(const Context &C);
+
 }  // namespace gcs
 
 // The C handle (gamera_cs_b200.h): device arrays of one context's boundary.
-struct gcs_context;
 struct gcs_earth {
-  gcs_context *ctx = nullptr;
+  gcs::Context *C = nullptr;
   gcs::EarthDev dev{};
   void *pool = nullptr;          // geometry of the boundary layers
   void *wind_pool = nullptr;     // monitor time series

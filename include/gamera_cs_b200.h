@@ -379,6 +379,31 @@ int gcs_context_precision(const gcs_context *ctx);
 int gcs_context_set_bulk_threshold(gcs_context *ctx, double b0_threshold);
 int gcs_context_bulk_split(const gcs_context *ctx);
 
+/* The reference's Earth radial-boundary callbacks
+ * (cubedsphere/cubedsphere_earth_boundary.h:26-52), same signatures and
+ * results.  Passed to the drop-in step (radial_boundary =
+ * gamera_cs_earth_fill_radial_ghosts with options->fluid_flux_sync =
+ * gamera_cs_earth_inner_fluid_flux, options->edge_emf_sync =
+ * gamera_cs_earth_no_mi_emf and the same boundary as both contexts), they
+ * run as device kernels inside the step with no host round trip unless the
+ * boundary's MI coupling is ready; called directly they work on host
+ * storage (the radial fill through the grid's device context). */
+int gamera_cs_earth_fill_radial_ghosts(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                       gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                       const size_t active[3], size_t ghost,
+                                       double current_time, double previous_time,
+                                       void *context);
+int gamera_cs_earth_fill_radial_ghosts_face(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
+                                            gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
+                                            const size_t active[3], size_t ghost,
+                                            double current_time, double previous_time,
+                                            void *context, int face);
+int gamera_cs_earth_inner_fluid_flux(gamera_no_storage *storage, const gamera_no_grid *grid,
+                                     const size_t lower[3], const size_t upper[3],
+                                     void *context);
+int gamera_cs_earth_no_mi_emf(gamera_no_storage *storage, const gamera_no_grid *grid,
+                              const size_t lower[3], const size_t upper[3], void *context);
+
 /* Device Earth radial boundary (no-MI wall) of a context made from a host
  * grid: the reference callbacks gamera_cs_earth_fill_radial_ghosts
  * (radial ghost cells and faces of the state and old state at both shells,

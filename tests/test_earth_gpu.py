@@ -153,3 +153,102 @@ def test_earth_boundary_rejects_bad_input(lib):
     finally:
         lib.gcs_context_destroy(ctx)
         case.close()
+
+
+def earth_options(cbs, case, b):
+    o = abi.AdvanceOptions.from_buffer_copy(case.options.contents)
+    o.fluid_flux_sync = C.cast(cbs.gamera_cs_earth_inner_fluid_flux, C.c_void_p).value
+    o.edge_emf_sync = C.cast(cbs.gamera_cs_earth_no_mi_emf, C.c_void_p).value
+    o.edge_emf_context = C.cast(C.pointer(b), C.c_void_p).value
+    return o
+
+
+@pytest.mark.parametrize("strict", [0, 1])
+def test_drop_in_step_with_earth_callbacks(lib, strict):
+    """A reference caller's unchanged Earth-driver step (the reference's
+    callback symbols, resolved in this library) against the reference."""
+    if not refbind.ref_available():
+        pytest.skip("reference library not built")
+    R = refbind.ref()
+    abi.bind(R, abi.earth_callback_signatures())
+    ref = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    gpu = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    keep = []
+    startup = abi.EarthStartup()
+    startup.gamma = 5.0 / 3.0
+    wind = wind_series(keep)
+    b_ref = boundary(startup, wind, ref.background, strict)
+    b_gpu = boundary(startup, wind, gpu.background, strict)
+    ropts, gopts = earth_options(R, ref, b_ref), earth_options(lib, gpu, b_gpu)
+    plan = C.c_void_p()
+    assert lib.gamera_cs_halo_plan_create(gpu.grid, gpu.active, gpu.ghost, C.byref(plan)) == 0
+    try:
+        time, dt_prev = 0.0, 0.0
+        for s in range(3):
+            local = ref.local_timestep()
+            dt = 0.5 * local if dt_prev == 0.0 else min(0.5 * local, 1.25 * dt_prev)
+            ratio = 0.0 if dt_prev == 0.0 else 0.5 * dt / dt_prev
+            prev = time if s == 0 else time - dt_prev
+            for bd in (b_ref, b_gpu):
+                bd.step_time, bd.step_dt = time, dt
+            assert R.gamera_cs_advance_six_with_background_planned(
+                ref.grid, ref.storage, ref.active, ref.ghost, ratio, dt, C.byref(ropts),
+                ref.background, R.fx_plan(ref.handle),
+                C.cast(R.gamera_cs_earth_fill_radial_ghosts, C.c_void_p),
+                time, prev, C.cast(C.pointer(b_ref), C.c_void_p)) == 0
+            assert lib.gamera_cs_advance_six_with_background_planned(
+                gpu.grid, gpu.storage, gpu.active, gpu.ghost, ratio, dt, C.byref(gopts),
+                gpu.background, plan, C.cast(lib.gamera_cs_earth_fill_radial_ghosts,
+                                             C.c_void_p),
+                time, prev, C.cast(C.pointer(b_gpu), C.c_void_p)) == 0
+            res = compare_state(gpu, ref, NAMES)
+            bad = {k: v for k, v in res.items() if not v[0] <= 1e-12 * 10 ** s}
+            assert not bad, "step %d: %s" % (s, bad)
+            time += dt
+            dt_prev = dt
+    finally:
+        lib.gamera_cs_halo_plan_destroy(plan)
+        ref.close()
+        gpu.close()
+
+
+def test_direct_radial_fill_matches_reference(lib):
+    """gamera_cs_earth_fill_radial_ghosts called on host storage (all faces,
+    then one receiver face) against the reference's."""
+    if not refbind.ref_available():
+        pytest.skip("reference library not built")
+    R = refbind.ref()
+    abi.bind(R, abi.earth_callback_signatures())
+    ref = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    gpu = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    one = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    keep = []
+    startup = abi.EarthStartup()
+    startup.gamma = 5.0 / 3.0
+    wind = wind_series(keep)
+    try:
+        for case, fn in ((ref, R), (gpu, lib)):
+            bd = boundary(startup, wind, case.background, 0)
+            keep.append(bd)
+            assert fn.gamera_cs_earth_fill_radial_ghosts(case.grid, case.storage, case.active,
+                                                         case.ghost, 0.006, 0.002,
+                                                         C.byref(bd)) == 0
+        res = compare_state(gpu, ref, NAMES)
+        bad = {k: v for k, v in res.items() if not v[0] <= 1e-12}
+        assert not bad, bad
+        bd = boundary(startup, wind, one.background, 0)
+        before = [one.arrays(f)["conserved"].copy() for f in range(6)]
+        assert lib.gamera_cs_earth_fill_radial_ghosts_face(one.grid, one.storage, one.active,
+                                                           one.ghost, 0.006, 0.002,
+                                                           C.byref(bd), 2) == 0
+        for f in range(6):
+            now = one.arrays(f)["conserved"]
+            if f == 2:
+                np.testing.assert_allclose(now, ref.arrays(2)["conserved"], rtol=0,
+                                           atol=1e-12 * np.max(np.abs(now)))
+            else:
+                np.testing.assert_array_equal(now, before[f])
+    finally:
+        ref.close()
+        gpu.close()
+        one.close()

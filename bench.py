@@ -279,6 +279,7 @@ def run_gpu(args):
 
     mi_solo = run_mi(lib, torch, device, args.mi_solves) if args.mi_solves > 0 else None
     bulk = run_bulk(lib, torch, device, args, dist) if args.bulk else None
+    earth = run_earth(lib, torch, device, args, dist, ctx) if args.earth_steps > 0 else None
     # the ensemble needs most of the GPU's memory: free the production run first
     had_mi = mi is not None
     if mi is not None:
@@ -346,6 +347,8 @@ def run_gpu(args):
             result["fp32_bulk"] = bulk
         if ens is not None:
             result["ensemble"] = ens
+        if earth is not None:
+            result["earth_boundary"] = earth
         if args.cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(args)
             if mi_solo is not None:
@@ -399,6 +402,73 @@ def run_bulk(lib, torch, device, args, dist):
             "note": "flux/face-velocity/EMF sweeps in FP32 outside the layers "
                     "where |B0| > 8 (those stay FP64); state, face B, CT, "
                     "predictor and recovery FP64"}
+
+
+def run_earth(lib, torch, device, args, dist, ctx):
+    """The production case stepped with the device Earth radial boundary
+    (no-MI wall): radial ghosts from a constant upstream monitor (the case's
+    own wind), inner flux trap, wind-driven outer EMF, one
+    gcs_context_step_earth call per step (host-driven dt, no graph)."""
+    from gamera_cube_b200 import abi
+    opts, ts = abi.AdvanceOptions(), abi.TimestepOptions()
+    lib.gcs_case_options(KIND_WIND, C.byref(opts), C.byref(ts))
+    bnorm = 100000.0 * (4.0e-7 * 3.141592653589793 * 1.67262192369e-21) ** 0.5
+    st = (abi.SolarWindState * 1)()
+    st[0].density = 5.0
+    st[0].pressure = 5.0e6 * 1.380649e-23 * 1.0e5 / (1.67262192369e-21 * 1.0e10)
+    st[0].velocity[:] = [-4.0, 0.0, 0.0]
+    st[0].magnetic[:] = [0.0, 0.0, -5.0e-9 / bnorm]
+    t0 = (C.c_double * 1)(0.0)
+    wind = abi.SolarWindSeries()
+    wind.count, wind.time, wind.state = 1, t0, st
+    wind.reference[:] = [30.0, 0.0, 0.0]
+    wind.linear_interpolation = 1
+    startup = abi.EarthStartup()
+    startup.gamma = 5.0 / 3.0
+    b = abi.EarthBoundary()
+    b.startup, b.wind = C.pointer(startup), C.pointer(wind)
+    b.density_floor, b.pressure_floor, b.cfl = 1e-6, 1e-8, 0.3
+    earth = C.c_void_p()
+    if lib.gcs_earth_create_case(ctx, C.byref(b), C.byref(earth)) != 0:
+        return {"error": lib.gcs_last_error().decode()}
+    stream = torch.cuda.ExternalStream(lib.gcs_context_stream(ctx), device=device)
+    local = C.c_double()
+    lib.gcs_context_timestep(ctx, C.byref(ts), C.byref(local))
+    dt = 0.5 * local.value
+    clock = [0.0]
+
+    def steps(k):
+        for _ in range(k):
+            prev = clock[0] - dt if clock[0] > 0.0 else clock[0]
+            if lib.gcs_context_step_earth(ctx, earth, C.byref(opts), 0.5 if clock[0] > 0 else 0.0,
+                                          dt, clock[0], prev) != 0:
+                return False
+            clock[0] += dt
+        return True
+
+    ok = steps(3)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    start.record(stream)
+    ok = ok and steps(args.earth_steps)
+    stop.record(stream)
+    stop.synchronize()
+    ms = max_over_ranks(start.elapsed_time(stop), dist, device)
+    act = (C.c_size_t * 3)()
+    g = C.c_size_t()
+    lib.gcs_context_dims(ctx, act, C.byref(g))
+    cells = 6 * act[0] * act[1] * act[2]
+    total = sum_over_ranks(float(cells), dist, device)
+    nbytes = lib.gcs_earth_device_bytes(earth)
+    lib.gcs_earth_destroy(earth)
+    return {"value": total * args.earth_steps / (ms * 1e-3), "unit": "cell-updates/s",
+            "ms_per_step": ms / args.earth_steps, "steps": args.earth_steps, "ok": bool(ok),
+            "workload": "6 x %dx%dx%d wind + dipole, device Earth radial boundary (no-MI wall), "
+                        "constant upstream monitor" % (act[1], act[2], act[0]),
+            "call": "gcs_context_step_earth (host-driven step, status read back each step)",
+            "boundary_device_bytes": nbytes,
+            "gpu_launches_per_step": 22 + 19}
 
 
 ENS_SEED = 2024
@@ -779,6 +849,8 @@ def main():
                     help="timed ionosphere solves (0 skips the MI measurement)")
     ap.add_argument("--no-bulk", dest="bulk", action="store_false",
                     help="skip the FP32-bulk variant measurement")
+    ap.add_argument("--earth-steps", type=int, default=20,
+                    help="timed steps with the device Earth boundary (0 skips them)")
     ap.add_argument("--ens-steps", type=int, default=20,
                     help="timed steps of the 16-run ensemble (0 skips it)")
     ap.add_argument("--ens-warmup", type=int, default=3)

@@ -283,9 +283,11 @@ def ensemble_signatures():
         "gcs_ensemble_graph_info": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int)]),
         "gcs_earth_create": (C.c_int, [C.c_void_p, P(Grid), P(EarthBoundary),
                                        P(C.c_void_p)]),
+        "gcs_earth_create_case": (C.c_int, [C.c_void_p, P(EarthBoundary), P(C.c_void_p)]),
         "gcs_earth_set_wind": (C.c_int, [C.c_void_p, P(SolarWindSeries)]),
         "gcs_earth_destroy": (None, [C.c_void_p]),
         "gcs_earth_device_bytes": (C.c_size_t, [C.c_void_p]),
+        "gcs_earth_copy_layers": (C.c_size_t, [C.c_void_p, C.c_void_p, C.c_size_t]),
         "gcs_context_step_earth": (C.c_int, [C.c_void_p, C.c_void_p, P(AdvanceOptions),
                                              C.c_double, C.c_double, C.c_double,
                                              C.c_double]),

@@ -327,21 +327,16 @@ __global__ void k_cell_centroids(Dims D, const gamera_no_cell_geometry *cells,
 
 // Edge frames of family e (nonorthogonal_grid.c:129-210,
 // nonorthogonal_geometry.c:245-262).
-__global__ void k_edges(Dims D, int f, int e, const V3 *vert, DevGeom G,
-                        int *bad) {
-  const int e0 = D.E0 + (e != 0), e1 = D.E1 + (e != 1), e2 = D.E2 + (e != 2);
-  const long long t = tid();
-  if (t >= (long long)e0 * e1 * e2) return;
-  const int i = (int)(t / ((long long)e1 * e2));
-  const int j = (int)((t / e2) % e1);
-  const int k = (int)(t % e2);
-  const long long c = f * D.Nn + D.node(i, j, k);
+// Frame of edge (i, j, k) of family e from the vertices: 0 on success, 1
+// for an edge on the boundary of the extent (no frame), 2 for a degenerate
+// edge.
+__device__ int edge_frame(const Dims &D, int e, const V3 *vert, int i, int j, int k,
+                          V3 *nrm, V3 *t1, V3 *t2, double *len) {
   int interior;
   if (e == 0) interior = j > 0 && j < D.E1 && k > 0 && k < D.E2;
   else if (e == 1) interior = i > 0 && i < D.E0 && k > 0 && k < D.E2;
   else interior = i > 0 && i < D.E0 && j > 0 && j < D.E1;
-  G.edge_ok[e][c] = (unsigned char)kStageEdgeGeometry;
-  if (!interior) return;
+  if (!interior) return 1;
   const int V1 = D.E1 + 1, V2 = D.E2 + 1;
   auto vx = [&](int a, int b, int q) {
     return vert[((long long)a * V1 + b) * V2 + q];
@@ -361,10 +356,30 @@ __global__ void k_edges(Dims D, int f, int e, const V3 *vert, DevGeom G,
   }
   const V3 avg = vscale(vadd(first, second), 0.5);
   const V3 ed = vsub(vx(en[0], en[1], en[2]), vx(i, j, k));
-  const double len = sqrt(vdot(ed, ed));
+  *len = sqrt(vdot(ed, ed));
+  if (!isfinite(*len) || *len <= DBL_MIN || !normalize(ed, nrm) ||
+      !normalize(vcross(avg, *nrm), t1) || !normalize(vcross(*nrm, *t1), t2))
+    return 2;
+  return 0;
+}
+
+// Edge frames of family e (nonorthogonal_grid.c:129-210,
+// nonorthogonal_geometry.c:245-262).
+__global__ void k_edges(Dims D, int f, int e, const V3 *vert, DevGeom G,
+                        int *bad) {
+  const int e0 = D.E0 + (e != 0), e1 = D.E1 + (e != 1), e2 = D.E2 + (e != 2);
+  const long long t = tid();
+  if (t >= (long long)e0 * e1 * e2) return;
+  const int i = (int)(t / ((long long)e1 * e2));
+  const int j = (int)((t / e2) % e1);
+  const int k = (int)(t % e2);
+  const long long c = f * D.Nn + D.node(i, j, k);
+  G.edge_ok[e][c] = (unsigned char)kStageEdgeGeometry;
   V3 nrm, t1, t2;
-  if (!isfinite(len) || len <= DBL_MIN || !normalize(ed, &nrm) ||
-      !normalize(vcross(avg, nrm), &t1) || !normalize(vcross(nrm, t1), &t2)) {
+  double len;
+  const int r = edge_frame(D, e, vert, i, j, k, &nrm, &t1, &t2, &len);
+  if (r == 1) return;
+  if (r == 2) {
     atomicExch(bad, 1);
     return;
   }
@@ -376,6 +391,64 @@ __global__ void k_edges(Dims D, int f, int e, const V3 *vert, DevGeom G,
   G.et2[e][1][c] = t2.y;
   G.et2[e][2][c] = t2.z;
   G.edge_ok[e][c] = 0;
+}
+
+// Geometry of the radial boundary layers for the device Earth boundary,
+// on the node plane of each face (layouts of gcs_earth.h).
+__global__ void k_earth_layer_cells(Dims D, int f, const gamera_no_cell_geometry *cells,
+                                    EarthLayers L) {
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= D.E1 * D.E2) return;
+  const int l = blockIdx.y, j = jk / D.E2, k = jk % D.E2;
+  const int i = l < D.g ? l : D.g + D.nr + (l - D.g);
+  const gamera_no_vec3 x = cells[((long long)i * D.E1 + j) * D.E2 + k].centroid;
+  const long long q = (((long long)f * 2 * D.g + l) * D.N1 + j) * D.N2 + k;
+  for (int c = 0; c < 3; ++c) L.cell_cen[c][q] = x.value[c];
+}
+
+__global__ void k_earth_layer_faces(Dims D, int f, int d, const gamera_no_vec3 *cen,
+                                    const gamera_no_vec3 *av, DevGeom G, DevBg B,
+                                    EarthLayers L) {
+  const int e1 = D.E1 + (d == 1), e2 = D.E2 + (d == 2);
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= e1 * e2) return;
+  const int l = blockIdx.y, j = jk / e2, k = jk % e2;
+  const int i = D.g + D.nr + (d == 0) + l;
+  const long long s = ((long long)i * e1 + j) * e2 + k;
+  const long long q = (((long long)f * D.g + l) * D.N1 + j) * D.N2 + k;
+  const long long c = f * D.Nn + D.node(i, j, k);
+  for (int a = 0; a < 3; ++a) {
+    L.face_cen[d][a][q] = cen[s].value[a];
+    L.face_av[d][a][q] = av[s].value[a];
+  }
+  L.face_bg[d][q] = B.fb0n[d][c] * G.area[d][c];
+}
+
+__global__ void k_earth_layer_edges(Dims D, int f, int e, const V3 *vert, EarthLayers L) {
+  const int e1 = D.E1 + (e != 1), e2 = D.E2 + (e != 2);
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= e1 * e2) return;
+  const int l = blockIdx.y, j = jk / e2, k = jk % e2;
+  const int i = l == 0 ? D.g : D.g + D.nr - 3 + (l - 1);
+  const long long q = (((long long)f * 5 + l) * D.N1 + j) * D.N2 + k;
+  L.edge_valid[e][q] = 0;
+  if (i >= D.E0 + (e != 0)) return;
+  const int V1 = D.E1 + 1, V2 = D.E2 + 1;
+  int up[3] = {i, j, k};
+  ++up[e];
+  const V3 a = vert[((long long)i * V1 + j) * V2 + k];
+  const V3 z = vert[((long long)up[0] * V1 + up[1]) * V2 + up[2]];
+  L.edge_mid[e][0][q] = 0.5 * (a.x + z.x);
+  L.edge_mid[e][1][q] = 0.5 * (a.y + z.y);
+  L.edge_mid[e][2][q] = 0.5 * (a.z + z.z);
+  V3 nrm, t1, t2;
+  double len;
+  if (edge_frame(D, e, vert, i, j, k, &nrm, &t1, &t2, &len) != 0) return;
+  L.edge_nrm[e][0][q] = nrm.x;
+  L.edge_nrm[e][1][q] = nrm.y;
+  L.edge_nrm[e][2][q] = nrm.z;
+  L.edge_len[e][q] = len;
+  L.edge_valid[e][q] = 1;
 }
 
 // Dipole B = 3 (m.r) r / r^5 - m / r^3 (nonorthogonal_background.c:422-442).
@@ -903,6 +976,58 @@ int Context::init_member(Context &o, unsigned long long seed, const WindInit &w)
   cudaFree(work);
   if (hbad) {
     set_error("degenerate geometry or invalid initial state", "init_member");
+    return -1;
+  }
+  return 0;
+}
+
+// Boundary-layer geometry of the device Earth boundary for a device-built
+// wind case: vertices, cells and faces of each face rebuilt into scratch,
+// the radial boundary layers copied into L, outer faces' B0 flux from the
+// background (flux / area x area).
+int Context::build_earth_layers(const EarthLayers &L) {
+  if (owner || !staging || !bg_pool) {
+    set_error("needs a device-built wind case", "build_earth_layers");
+    return -1;
+  }
+  const Dims &D = X.D;
+  const long long cells = (long long)D.E0 * D.E1 * D.E2;
+  const long long verts = (long long)(D.E0 + 1) * (D.E1 + 1) * (D.E2 + 1);
+  const size_t fmax = (size_t)verts;
+  void *work = nullptr;
+  const size_t wbytes = verts * sizeof(V3) + 2 * fmax * sizeof(gamera_no_vec3) + sizeof(int);
+  GCS_BTRY(cudaMalloc(&work, wbytes));
+  V3 *vert = (V3 *)work;
+  gamera_no_vec3 *cen = (gamera_no_vec3 *)(vert + verts);
+  gamera_no_vec3 *av = cen + fmax;
+  int *bad = (int *)(av + fmax);
+  GCS_BTRY(cudaMemsetAsync(bad, 0, sizeof(int), stream));
+  gamera_no_cell_geometry *acells = (gamera_no_cell_geometry *)staging;
+  const int bs = 128;
+  for (int f = 0; f < kFaces; ++f) {
+    k_vertices<<<nblk(verts, bs), bs, 0, stream>>>(f, D.nr, D.n, D.g, 2.5, 30.0,
+                                                   log(12.0), vert);
+    k_cells<<<nblk(cells, 64), 64, 0, stream>>>(D, vert, acells, bad);
+    k_earth_layer_cells<<<dim3(nblk((long long)D.E1 * D.E2, bs), 2 * D.g), bs, 0,
+                          stream>>>(D, f, acells, L);
+    for (int d = 0; d < 3; ++d) {
+      const long long fc = (long long)(D.E0 + (d == 0)) * (D.E1 + (d == 1)) *
+                           (D.E2 + (d == 2));
+      k_faces_from_cells<<<nblk(fc, bs), bs, 0, stream>>>(D, f, d, acells, X.G, cen, av);
+      const long long pl = (long long)(D.E1 + (d == 1)) * (D.E2 + (d == 2));
+      k_earth_layer_faces<<<dim3(nblk(pl, bs), D.g), bs, 0, stream>>>(D, f, d, cen, av, X.G,
+                                                                      X.BG, L);
+      const long long pe = (long long)(D.E1 + (d != 1)) * (D.E2 + (d != 2));
+      k_earth_layer_edges<<<dim3(nblk(pe, bs), 5), bs, 0, stream>>>(D, f, d, vert, L);
+    }
+    GCS_BTRY(cudaGetLastError());
+    GCS_BTRY(cudaStreamSynchronize(stream));
+  }
+  int hbad = 0;
+  GCS_BTRY(cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(work);
+  if (hbad) {
+    set_error("degenerate boundary-layer geometry", "build_earth_layers");
     return -1;
   }
   return 0;

@@ -65,6 +65,9 @@ struct Context {
   // (gcs_build.cu); no host grid is involved.
   int init_case(int kind, size_t nr, size_t n, unsigned long long seed,
                 const WindInit *driver = nullptr);
+  // Radial boundary-layer geometry of a device-built wind case for the
+  // device Earth boundary (gcs_build.cu).
+  int build_earth_layers(const EarthLayers &L);
   // A wind run on the grid of `o` with its own state (gcs_build.cu).
   int init_member(Context &o, unsigned long long seed, const WindInit &w);
   // Non-null for a run sharing the grid of another context; only the state

@@ -100,6 +100,15 @@ struct WindInit {
   int pulse;
 };
 
+// Writable view of the Earth boundary-layer geometry (layouts of
+// gcs_earth.h), filled by the device case builder.
+struct EarthLayers {
+  double *cell_cen[3];
+  double *face_cen[3][3], *face_av[3][3], *face_bg[3];
+  double *edge_mid[3][3], *edge_nrm[3][3], *edge_len[3];
+  unsigned char *edge_valid[3];
+};
+
 // Scalar parameters of one step.  dt and ratio live in device memory so a
 // captured CUDA graph can advance its own time step.
 struct StepParams {

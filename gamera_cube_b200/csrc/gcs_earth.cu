@@ -504,6 +504,55 @@ int upload_wind(gcs_earth *e, const gamera_solar_wind_series *w) {
   return 0;
 }
 
+// Counts of the boundary-layer arrays (layouts of gcs_earth.h).
+void earth_counts(const gcs::Dims &D, long long *ncell, long long *nface, long long *nedge,
+                  long long *doubles) {
+  const long long P = (long long)D.N1 * D.N2;
+  *ncell = 6LL * 2 * D.g * P;
+  *nface = 6LL * D.g * P;
+  *nedge = 6LL * 5 * P;
+  *doubles = 3 * *ncell + 3 * 7 * *nface + 3 * 7 * *nedge;
+}
+
+// Point the boundary's device arrays into its pool: cell centroids, then per
+// face family centroid[3], area vector[3], B0 flux, then per edge family
+// midpoint[3], direction[3], length, then the edge validity bytes.
+gcs::EarthLayers earth_bind(gcs_earth *e, const gcs::Dims &D) {
+  long long ncell, nface, nedge, doubles;
+  earth_counts(D, &ncell, &nface, &nedge, &doubles);
+  double *dp = (double *)e->pool;
+  unsigned char *vp = (unsigned char *)e->pool + doubles * sizeof(double);
+  gcs::EarthLayers L;
+  for (int c = 0; c < 3; ++c) L.cell_cen[c] = dp + c * ncell;
+  double *fp = dp + 3 * ncell;
+  double *ep = fp + 3 * 7 * nface;
+  for (int d = 0; d < 3; ++d) {
+    for (int c = 0; c < 3; ++c) {
+      L.face_cen[d][c] = fp + (d * 7 + c) * nface;
+      L.face_av[d][c] = fp + (d * 7 + 3 + c) * nface;
+      L.edge_mid[d][c] = ep + (d * 7 + c) * nedge;
+      L.edge_nrm[d][c] = ep + (d * 7 + 3 + c) * nedge;
+    }
+    L.face_bg[d] = fp + (d * 7 + 6) * nface;
+    L.edge_len[d] = ep + (d * 7 + 6) * nedge;
+    L.edge_valid[d] = vp + d * nedge;
+  }
+  gcs::EarthDev &E = e->dev;
+  for (int c = 0; c < 3; ++c) E.cell_cen[c] = L.cell_cen[c];
+  for (int d = 0; d < 3; ++d) {
+    for (int c = 0; c < 3; ++c) {
+      E.face_cen[d][c] = L.face_cen[d][c];
+      E.face_av[d][c] = L.face_av[d][c];
+      E.edge_mid[d][c] = L.edge_mid[d][c];
+      E.edge_nrm[d][c] = L.edge_nrm[d][c];
+    }
+    E.face_bg[d] = L.face_bg[d];
+    E.edge_len[d] = L.edge_len[d];
+    E.edge_valid[d] = L.edge_valid[d];
+  }
+  return L;
+}
+
 int earth_create(gcs::Context &C, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
                  const gamera_cs_earth_boundary *b, gcs_earth **out,
                  bool allow_mi = false) {
@@ -538,10 +587,9 @@ int earth_create(gcs::Context &C, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT
   gcs_earth *e = new (std::nothrow) gcs_earth;
   if (!e) return -1;
   e->C = &C;
-  const long long P = (long long)D.N1 * D.N2;
   const int g = D.g, outer = D.g + D.nr;
-  const long long ncell = 6LL * 2 * g * P, nface = 6LL * g * P, nedge = 6LL * 5 * P;
-  const long long doubles = 3 * ncell + 3 * 7 * nface + 3 * 7 * nedge;
+  long long ncell, nface, nedge, doubles;
+  earth_counts(D, &ncell, &nface, &nedge, &doubles);
   std::vector<double> h(doubles, 0.0);
   std::vector<unsigned char> hv(3 * nedge, 0);
   double *cell = h.data();
@@ -612,23 +660,8 @@ int earth_create(gcs::Context &C, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT
     gcs::set_api_error("cannot upload the Earth boundary geometry");
     return -1;
   }
-  const double *dp = (const double *)e->pool;
-  const unsigned char *vp = (const unsigned char *)e->pool + doubles * sizeof(double);
+  earth_bind(e, D);
   gcs::EarthDev &E = e->dev;
-  for (int c = 0; c < 3; ++c) E.cell_cen[c] = dp + c * ncell;
-  const double *fp = dp + 3 * ncell;
-  const double *ep = fp + 3 * 7 * nface;
-  for (int d = 0; d < 3; ++d) {
-    for (int c = 0; c < 3; ++c) {
-      E.face_cen[d][c] = fp + (d * 7 + c) * nface;
-      E.face_av[d][c] = fp + (d * 7 + 3 + c) * nface;
-      E.edge_mid[d][c] = ep + (d * 7 + c) * nedge;
-      E.edge_nrm[d][c] = ep + (d * 7 + 3 + c) * nedge;
-    }
-    E.face_bg[d] = fp + (d * 7 + 6) * nface;
-    E.edge_len[d] = ep + (d * 7 + 6) * nedge;
-    E.edge_valid[d] = vp + d * nedge;
-  }
   E.gamma = b->startup->gamma;
   E.rho_floor = b->density_floor;
   E.p_floor = b->pressure_floor;
@@ -983,6 +1016,54 @@ int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_
   return earth_create(ctx->c, grid, b, out);
 }
 
+int gcs_earth_create_case(gcs_context *ctx, const gamera_cs_earth_boundary *b,
+                          gcs_earth **out) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (!ctx || !b || !b->startup || !b->wind || b->wind->count < 1 || !b->wind->time ||
+      !b->wind->state || !std::isfinite(b->density_floor) || !(b->density_floor > 0.0) ||
+      !std::isfinite(b->pressure_floor) || !(b->pressure_floor > 0.0) ||
+      !(b->cfl > 0.0) || !std::isfinite(b->startup->gamma)) {
+    gcs::set_api_error("invalid Earth boundary");
+    return -1;
+  }
+  if (b->mi != nullptr && gamera_cs_mi_dipole_ready(b->mi)) {
+    gcs::set_api_error("the MI-coupled inner wall needs the host callback path");
+    return -1;
+  }
+  gcs::Context &C = ctx->c;
+  gcs_earth *e = new (std::nothrow) gcs_earth;
+  if (!e) return -1;
+  e->C = &C;
+  long long ncell, nface, nedge, doubles;
+  earth_counts(C.X.D, &ncell, &nface, &nedge, &doubles);
+  e->pool_bytes = doubles * sizeof(double) + 3 * nedge;
+  if (cudaMalloc(&e->pool, e->pool_bytes) != cudaSuccess ||
+      cudaMemset(e->pool, 0, e->pool_bytes) != cudaSuccess) {
+    gcs_earth_destroy(e);
+    gcs::set_api_error("cannot allocate the Earth boundary geometry");
+    return -1;
+  }
+  const gcs::EarthLayers L = earth_bind(e, C.X.D);
+  if (C.build_earth_layers(L) != 0) {
+    gcs::set_api_error(C.error);
+    gcs_earth_destroy(e);
+    return -1;
+  }
+  gcs::EarthDev &E = e->dev;
+  E.gamma = b->startup->gamma;
+  E.rho_floor = b->density_floor;
+  E.p_floor = b->pressure_floor;
+  E.cfl = b->cfl;
+  E.strict_wall = b->strict_inner_gas_wall;
+  if (upload_wind(e, b->wind) != 0) {
+    gcs_earth_destroy(e);
+    return -1;
+  }
+  *out = e;
+  return 0;
+}
+
 int gcs_earth_set_wind(gcs_earth *earth, const gamera_solar_wind_series *wind) {
   if (!earth) return -1;
   if (cudaStreamSynchronize(earth->C->stream) != cudaSuccess) return -1;
@@ -995,6 +1076,14 @@ void gcs_earth_destroy(gcs_earth *earth) {
   if (earth->pool) cudaFree(earth->pool);
   if (earth->wind_pool) cudaFree(earth->wind_pool);
   delete earth;
+}
+
+size_t gcs_earth_copy_layers(const gcs_earth *earth, void *host, size_t capacity) {
+  if (!earth || !earth->pool) return 0;
+  if (host && capacity >= earth->pool_bytes &&
+      cudaMemcpy(host, earth->pool, earth->pool_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return 0;
+  return earth->pool_bytes;
 }
 
 size_t gcs_earth_device_bytes(const gcs_earth *earth) {

@@ -417,10 +417,22 @@ int gamera_cs_earth_no_mi_emf(gamera_no_storage *storage, const gamera_no_grid *
 typedef struct gcs_earth gcs_earth;
 int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
                      const gamera_cs_earth_boundary *boundary, gcs_earth **earth);
+/* The same for a device-built wind case (gcs_context_create_case kind 2/3,
+ * gcs_context_create_wind): the boundary layers' geometry is rebuilt on the
+ * device and the outer faces' B0 flux taken from the context's background
+ * (boundary->background may be NULL). */
+int gcs_earth_create_case(gcs_context *ctx, const gamera_cs_earth_boundary *boundary,
+                          gcs_earth **earth);
 /* Replace the monitor time series (e.g. a longer one). */
 int gcs_earth_set_wind(gcs_earth *earth, const gamera_solar_wind_series *wind);
 void gcs_earth_destroy(gcs_earth *earth);
 size_t gcs_earth_device_bytes(const gcs_earth *earth);
+/* Diagnostics: copy the boundary-layer geometry (cell centroids; per face
+ * family outer ghost-face centroids, area vectors, B0 flux; per edge family
+ * midpoints, directions, lengths; edge validity bytes; node-plane layout of
+ * 2g, g and 5 layers per face) to `host` when capacity suffices; returns
+ * its size in bytes. */
+size_t gcs_earth_copy_layers(const gcs_earth *earth, void *host, size_t capacity);
 /* One step on the device-resident state with the device Earth boundary:
  * gamera_cs_advance_six_with_background_planned(..., radial_boundary =
  * gamera_cs_earth_fill_radial_ghosts, current_time, previous_time,

@@ -252,3 +252,62 @@ def test_direct_radial_fill_matches_reference(lib):
         ref.close()
         gpu.close()
         one.close()
+
+
+def test_device_built_case_boundary_matches_host_grid(lib):
+    """gcs_earth_create_case (boundary layers rebuilt on the device) against
+    gcs_earth_create on the oracle's host grid of the same case: one Earth
+    step agrees to the builders' level (1e-11).  As in the builder test,
+    conserved ghost values are compared on active cells: the cube-corner
+    diagonal ghosts take their donor by a projection tie that last-bit
+    differences of the device-built centroids flip, and later steps carry
+    that difference inward, in the plain step as well."""
+    from oracle import oracle_cases
+    host = oracle_cases.Case("wind", 12, 10, 7)
+    keep = []
+    startup = abi.EarthStartup()
+    startup.gamma = 5.0 / 3.0
+    wind = wind_series(keep)
+    b_host = boundary(startup, wind, host.background, 0)
+    b_dev = boundary(startup, wind, None, 0)
+    opts = abi.AdvanceOptions.from_buffer_copy(host.options.contents)
+    a = lib.gcs_context_create(host.grid, host.active, host.ghost)
+    d = lib.gcs_context_create_case(2, 12, 10, 7)
+    ea, ed = C.c_void_p(), C.c_void_p()
+    try:
+        assert a and d
+        assert lib.gcs_context_upload_background(a, host.background) == 0
+        assert lib.gcs_context_upload_state(a, host.storage) == 0
+        assert lib.gcs_earth_create(a, host.grid, C.byref(b_host), C.byref(ea)) == 0
+        assert lib.gcs_earth_create_case(d, C.byref(b_dev), C.byref(ed)) == 0, \
+            lib.gcs_last_error()
+        time, dt_prev = 0.0, 0.0
+        for s in range(1):
+            dt = 0.5 * host.local_timestep() if s == 0 else dt_prev
+            ratio = 0.0 if s == 0 else 0.5
+            prev = time if s == 0 else time - dt_prev
+            for ctx, e in ((a, ea), (d, ed)):
+                assert lib.gcs_context_step_earth(ctx, e, C.byref(opts), ratio, dt, time,
+                                                  prev) == 0
+            time += dt
+            dt_prev = dt
+        from tests.test_ensemble_gpu import download
+        ha, hd = download(lib, a), download(lib, d)
+        for name in ("conserved", "cell_magnetic", "face_flux0", "face_flux1", "face_flux2"):
+            worst = scale = 0.0
+            for f in range(6):
+                x, y = ha.arrays(f)[name], hd.arrays(f)[name]
+                g = host.ghost
+                if name == "conserved":   # corner-diagonal ghosts: donor ties
+                    x = x[g:-g, g:-g, g:-g]
+                    y = y[g:-g, g:-g, g:-g]
+                worst = max(worst, float(np.max(np.abs(x - y))))
+                scale = max(scale, float(np.max(np.abs(x))))
+            assert worst <= 1e-11 * scale, (name, worst / scale)
+    finally:
+        for e in (ea, ed):
+            if e:
+                lib.gcs_earth_destroy(e)
+        for ctx in (a, d):
+            if ctx:
+                lib.gcs_context_destroy(ctx)

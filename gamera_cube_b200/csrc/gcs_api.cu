@@ -392,20 +392,18 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
     return -1;
   C.reset_status_async();
   // The reference's Earth callbacks of this library run as device kernels
-  // inside the step (no host round trip) unless the MI coupling is ready.
+  // inside the step, with no host round trip.
   const gamera_cs_earth_boundary *eb = nullptr;
   if (grid != nullptr && radial == gamera_cs_earth_fill_radial_ghosts &&
       options->fluid_flux_sync == gamera_cs_earth_inner_fluid_flux &&
       options->edge_emf_sync == gamera_cs_earth_no_mi_emf &&
-      options->edge_emf_context == radial_ctx && radial_ctx != nullptr) {
+      options->edge_emf_context == radial_ctx && radial_ctx != nullptr)
     eb = (const gamera_cs_earth_boundary *)radial_ctx;
-    if (eb->mi != nullptr && gamera_cs_mi_dipole_ready(eb->mi)) eb = nullptr;
-  }
   int rc;
   if (eb != nullptr) {
     // the reference's EMF callback fails on these (cubedsphere_earth_boundary.c:388-389)
     if (!std::isfinite(eb->step_time) || !(eb->step_dt > 0.0)) return -1;
-    gcs_earth *earth = gcs::earth_for(C, grid, eb, false);
+    gcs_earth *earth = gcs::earth_for(C, grid, eb, true);
     if (earth == nullptr) return -1;
     const gcs::EarthStep es{&earth->dev, t, tprev, eb->step_time, eb->step_dt};
     rc = run_step(ctx, O, 0, nullptr, &es);
@@ -993,6 +991,7 @@ int gcs_context_step_earth(gcs_context *ctx, gcs_earth *earth,
                       C.stream) != cudaSuccess)
     return -1;
   C.reset_status_async();
+  if (gcs::earth_sync_mi(earth, earth->mi) != 0) return -1;
   // the reference driver sets step_time = current time, step_dt = dt
   // (test_cubedsphere_dipole_background.c:667-668)
   const gcs::EarthStep es{&earth->dev, current_time, previous_time, current_time, dt};

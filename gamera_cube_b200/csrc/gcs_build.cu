@@ -443,6 +443,15 @@ __global__ void k_earth_layer_edges(Dims D, int f, int e, const V3 *vert, EarthL
   L.edge_mid[e][2][q] = 0.5 * (a.z + z.z);
   V3 nrm, t1, t2;
   double len;
+  if (l == 0 && e > 0) {
+    const long long p = ((long long)f * D.N1 + j) * D.N2 + k;
+    L.inner_a[e - 1][0][p] = a.x;
+    L.inner_a[e - 1][1][p] = a.y;
+    L.inner_a[e - 1][2][p] = a.z;
+    L.inner_b[e - 1][0][p] = z.x;
+    L.inner_b[e - 1][1][p] = z.y;
+    L.inner_b[e - 1][2][p] = z.z;
+  }
   if (edge_frame(D, e, vert, i, j, k, &nrm, &t1, &t2, &len) != 0) return;
   L.edge_nrm[e][0][q] = nrm.x;
   L.edge_nrm[e][1][q] = nrm.y;

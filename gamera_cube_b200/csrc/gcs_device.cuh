@@ -107,6 +107,7 @@ struct EarthLayers {
   double *face_cen[3][3], *face_av[3][3], *face_bg[3];
   double *edge_mid[3][3], *edge_nrm[3][3], *edge_len[3];
   unsigned char *edge_valid[3];
+  double *inner_a[2][3], *inner_b[2][3];
 };
 
 // Scalar parameters of one step.  dt and ratio live in device memory so a

@@ -177,7 +177,17 @@ __global__ void k_earth_cells(Dims D, DevState S, EarthDev E, double time, int o
   }
   double v[3] = {p.vx, p.vy, p.vz};
   if (inner) {
-    if (E.strict_wall) {
+    if (E.mi) {
+      const gamera_no_vec3 pt = {{x[0], x[1], x[2]}};
+      const gamera_no_vec3 sv = {{v[0], v[1], v[2]}};
+      gamera_no_vec3 gv;
+      if (mi_ghost_velocity(E.mil, pt, sv, &gv) != 0) {
+        fail(st, kStageHost, 0, f, i, j, k);
+        return;
+      }
+      for (int c = 0; c < 3; ++c)
+        v[c] = E.strict_wall ? 0.5 * (gv.value[c] + v[c]) : gv.value[c];
+    } else if (E.strict_wall) {
       v[0] = v[1] = v[2] = 0.0;
     } else {
       double vn = 0.0;
@@ -395,15 +405,31 @@ __global__ void k_earth_emf_diffusive(Dims D, DevState S, DevGeom G, EarthDev E,
   S.E[2][c] += wtk * speed * cur_k * dl;
 }
 
-// E_t = 0 on the inner shell (cubedsphere_earth_boundary.c:428-437).
-__global__ void k_earth_emf_inner(Dims D, DevState S, EarthDev E, int d) {
+// E_t = 0 on the inner shell (cubedsphere_earth_boundary.c:428-437), or with
+// a ready MI coupling the potential difference along the edge
+// (cubedsphere_mi_dipole.c:478-503, applied after the zeroing at :438-441).
+__global__ void k_earth_emf_inner(Dims D, DevState S, EarthDev E, int d, DevStatus *st) {
   const int e1 = D.E1 + (d != 1), e2 = D.E2 + (d != 2);
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
   if (jk >= e1 * e2) return;
   const int f = blockIdx.z;
   const int j = jk / e2, k = jk % e2;
   if (!E.edge_valid[d][plane(D, f, 5, 0, j, k)]) return;
-  S.E[d][f * D.Nn + D.node(D.g, j, k)] = 0.0;
+  double emf = 0.0;
+  if (E.mi) {
+    const long long p = ((long long)f * D.N1 + j) * D.N2 + k;
+    const gamera_no_vec3 a = {{E.inner_a[d - 1][0][p], E.inner_a[d - 1][1][p],
+                               E.inner_a[d - 1][2][p]}};
+    const gamera_no_vec3 b = {{E.inner_b[d - 1][0][p], E.inner_b[d - 1][1][p],
+                               E.inner_b[d - 1][2][p]}};
+    double pa, pb;
+    if (mi_potential(E.mil, a, &pa) != 0 || mi_potential(E.mil, b, &pb) != 0) {
+      fail(st, kStageHost, d, f, D.g, j, k);
+      return;
+    }
+    emf = -(pb - pa) / E.mi_potential_norm;
+  }
+  S.E[d][f * D.Nn + D.node(D.g, j, k)] = emf;
 }
 
 inline unsigned blocks(long long n) { return (unsigned)((n + 127) / 128); }
@@ -448,7 +474,7 @@ void launch_earth_emf(const Ctx &X, const EarthDev &E, double step_time, double 
                           s>>>(D, X.S, X.G, E, tmid, step_dt, X.status);
   for (int d = 1; d < 3; ++d) {
     const long long pl = (long long)(D.E1 + (d != 1)) * (D.E2 + (d != 2));
-    k_earth_emf_inner<<<dim3(blocks(pl), 1, kFaces), 128, 0, s>>>(D, X.S, E, d);
+    k_earth_emf_inner<<<dim3(blocks(pl), 1, kFaces), 128, 0, s>>>(D, X.S, E, d, X.status);
   }
 }
 
@@ -511,7 +537,7 @@ void earth_counts(const gcs::Dims &D, long long *ncell, long long *nface, long l
   *ncell = 6LL * 2 * D.g * P;
   *nface = 6LL * D.g * P;
   *nedge = 6LL * 5 * P;
-  *doubles = 3 * *ncell + 3 * 7 * *nface + 3 * 7 * *nedge;
+  *doubles = 3 * *ncell + 3 * 7 * *nface + 3 * 7 * *nedge + 12 * 6LL * P;
 }
 
 // Point the boundary's device arrays into its pool: cell centroids, then per
@@ -537,7 +563,19 @@ gcs::EarthLayers earth_bind(gcs_earth *e, const gcs::Dims &D) {
     L.edge_len[d] = ep + (d * 7 + 6) * nedge;
     L.edge_valid[d] = vp + d * nedge;
   }
+  double *ip = ep + 3 * 7 * nedge;
+  const long long pl = 6LL * D.N1 * D.N2;
+  for (int d = 0; d < 2; ++d)
+    for (int c = 0; c < 3; ++c) {
+      L.inner_a[d][c] = ip + (d * 6 + c) * pl;
+      L.inner_b[d][c] = ip + (d * 6 + 3 + c) * pl;
+    }
   gcs::EarthDev &E = e->dev;
+  for (int d = 0; d < 2; ++d)
+    for (int c = 0; c < 3; ++c) {
+      E.inner_a[d][c] = L.inner_a[d][c];
+      E.inner_b[d][c] = L.inner_b[d][c];
+    }
   for (int c = 0; c < 3; ++c) E.cell_cen[c] = L.cell_cen[c];
   for (int d = 0; d < 3; ++d) {
     for (int c = 0; c < 3; ++c) {
@@ -564,10 +602,7 @@ int earth_create(gcs::Context &C, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT
     gcs::set_api_error("invalid Earth boundary");
     return -1;
   }
-  if (!allow_mi && b->mi != nullptr && gamera_cs_mi_dipole_ready(b->mi)) {
-    gcs::set_api_error("the MI-coupled inner wall needs the host callback path");
-    return -1;
-  }
+  (void)allow_mi;
   const gcs::Dims &D = C.X.D;
   for (int f = 0; f < gcs::kFaces; ++f) {
     const gamera_no_grid &g = grid[f];
@@ -646,6 +681,15 @@ int earth_create(gcs::Context &C, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT
               ed[(3 + c) * nedge + q] = eg.normal.value[c];
             }
             ed[6 * nedge + q] = eg.length;
+            if (l == 0 && d > 0) {
+              double *ip = edge + 3 * 7 * nedge;
+              const long long plane6 = 6LL * D.N1 * D.N2;
+              const long long p = ((long long)f * D.N1 + (long long)j) * D.N2 + (long long)k;
+              for (int c = 0; c < 3; ++c) {
+                ip[((d - 1) * 6 + c) * plane6 + p] = a.value[c];
+                ip[((d - 1) * 6 + 3 + c) * plane6 + p] = z.value[c];
+              }
+            }
           }
       }
     }
@@ -668,6 +712,11 @@ int earth_create(gcs::Context &C, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT
   E.cfl = b->cfl;
   E.strict_wall = b->strict_inner_gas_wall;
   if (upload_wind(e, b->wind) != 0) {
+    gcs_earth_destroy(e);
+    return -1;
+  }
+  e->mi = b->mi;
+  if (gcs::earth_sync_mi(e, e->mi) != 0) {
     gcs_earth_destroy(e);
     return -1;
   }
@@ -761,7 +810,41 @@ gcs_earth *earth_for(Context &C, const gamera_no_grid grid[kFaces],
   E.p_floor = b->pressure_floor;
   E.cfl = b->cfl;
   E.strict_wall = b->strict_inner_gas_wall;
+  if (earth_sync_mi(it->second.earth, allow_mi ? b->mi : nullptr) != 0) return nullptr;
   return it->second.earth;
+}
+
+int earth_sync_mi(gcs_earth *e, const gamera_cs_mi_dipole *mi) {
+  EarthDev &E = e->dev;
+  MiLookup L;
+  double norm;
+  if (mi == nullptr || !mi_lookup(mi, &L, &norm)) {
+    E.mi = 0;
+    return 0;
+  }
+  const size_t per = (size_t)L.np * (size_t)L.nt;
+  if (e->mi_count != 2 * per) {
+    if (e->mi_pot) cudaFree(e->mi_pot);
+    e->mi_pot = nullptr;
+    e->mi_count = 0;
+    if (cudaMalloc(&e->mi_pot, 2 * per * sizeof(double)) != cudaSuccess) {
+      set_api_error("cannot allocate the MI potential copy");
+      return -1;
+    }
+    e->mi_count = 2 * per;
+  }
+  // the previous step has finished: every step reads its status back
+  if (cudaStreamSynchronize(e->C->stream) != cudaSuccess) return -1;
+  for (int h = 0; h < 2; ++h)
+    if (cudaMemcpy(e->mi_pot + h * per, L.pot[h], per * sizeof(double),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return -1;
+  L.pot[0] = e->mi_pot;
+  L.pot[1] = e->mi_pot + per;
+  E.mil = L;
+  E.mi_potential_norm = norm;
+  E.mi = 1;
+  return 0;
 }
 
 void earth_forget(const Context &C) {
@@ -779,42 +862,6 @@ void earth_forget(const Context &C) {
 }  // namespace gcs
 
 namespace {
-
-// Inner ghost cells of one face with the MI drift velocity
-// (cubedsphere_earth_boundary.c:55-69), on host storage.
-int mi_inner_cells(const gamera_no_grid &grid, gamera_no_storage &st, size_t ghost,
-                   const gamera_cs_earth_boundary *b) {
-  const size_t *ex = grid.cell_extent;
-  for (int old = 0; old < 2; ++old) {
-    double *u = old ? st.old_conserved : st.conserved;
-    for (size_t i = 0; i < ghost; ++i)
-      for (size_t j = 0; j < ex[1]; ++j)
-        for (size_t k = 0; k < ex[2]; ++k) {
-          const size_t t = (i * ex[1] + j) * ex[2] + k;
-          const size_t s = ((2 * ghost - 1 - i) * ex[1] + j) * ex[2] + k;
-          gcs::Prim p;
-          if (gcs::cons_to_prim(&u[s * 5], b->startup->gamma, b->density_floor,
-                                b->pressure_floor, &p))
-            return -1;
-          const gamera_no_vec3 x = grid.cell[t].centroid;
-          const double radius = sqrt(x.value[0] * x.value[0] + x.value[1] * x.value[1] +
-                                     x.value[2] * x.value[2]);
-          if (!(radius > 0.0)) return -1;
-          const gamera_no_vec3 v = {{p.vx, p.vy, p.vz}};
-          gamera_no_vec3 gv;
-          if (gamera_cs_mi_dipole_ghost_velocity(b->mi, x, v, &gv) != 0) return -1;
-          if (b->strict_inner_gas_wall)
-            for (int c = 0; c < 3; ++c) gv.value[c] = 0.5 * (gv.value[c] + v.value[c]);
-          p.vx = gv.value[0];
-          p.vy = gv.value[1];
-          p.vz = gv.value[2];
-          if (gcs::prim_to_cons(p, b->startup->gamma, b->density_floor, b->pressure_floor,
-                                &u[t * 5]))
-            return -1;
-        }
-  }
-  return 0;
-}
 
 int fill_radial(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
                 gamera_no_storage storage[GAMERA_CS_FACE_COUNT], const size_t active[3],
@@ -846,8 +893,6 @@ int fill_radial(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
       if (C->transfer_array(f, gcs::kArrP, d, false, st.face_flux[d]) ||
           C->transfer_array(f, gcs::kArrPo, d, false, st.old_face_flux[d]))
         return -1;
-    if (b->mi && gamera_cs_mi_dipole_ready(b->mi) && mi_inner_cells(grid[f], st, ghost, b))
-      return -1;
   }
   return 0;
 }
@@ -1027,10 +1072,6 @@ int gcs_earth_create_case(gcs_context *ctx, const gamera_cs_earth_boundary *b,
     gcs::set_api_error("invalid Earth boundary");
     return -1;
   }
-  if (b->mi != nullptr && gamera_cs_mi_dipole_ready(b->mi)) {
-    gcs::set_api_error("the MI-coupled inner wall needs the host callback path");
-    return -1;
-  }
   gcs::Context &C = ctx->c;
   gcs_earth *e = new (std::nothrow) gcs_earth;
   if (!e) return -1;
@@ -1060,6 +1101,11 @@ int gcs_earth_create_case(gcs_context *ctx, const gamera_cs_earth_boundary *b,
     gcs_earth_destroy(e);
     return -1;
   }
+  e->mi = b->mi;
+  if (gcs::earth_sync_mi(e, e->mi) != 0) {
+    gcs_earth_destroy(e);
+    return -1;
+  }
   *out = e;
   return 0;
 }
@@ -1075,6 +1121,7 @@ void gcs_earth_destroy(gcs_earth *earth) {
   if (earth->C) cudaStreamSynchronize(earth->C->stream);
   if (earth->pool) cudaFree(earth->pool);
   if (earth->wind_pool) cudaFree(earth->wind_pool);
+  if (earth->mi_pot) cudaFree(earth->mi_pot);
   delete earth;
 }
 

@@ -7,6 +7,7 @@
 
 #include "gcs_kernels.cuh"
 #include "gamera_cs_types.h"
+#include "gcs_mi_lookup.cuh"
 
 struct gcs_earth;
 
@@ -33,9 +34,16 @@ struct EarthDev {
   const double *face_cen[3][3], *face_av[3][3], *face_bg[3];
   const double *edge_mid[3][3], *edge_nrm[3][3], *edge_len[3];
   const unsigned char *edge_valid[3];
+  // edge end points on the inner shell (i = g), edge families 1 and 2
+  const double *inner_a[2][3], *inner_b[2][3];
   WindDev wind;
   double gamma, rho_floor, p_floor, cfl;
   int strict_wall;
+  // ready MI coupling: inner ghost velocity from the E x B drift and the
+  // inner-shell EMF from the mapped potential (device copy in mil.pot)
+  int mi;
+  MiLookup mil;
+  double mi_potential_norm;
 };
 
 // Times of one step with the device Earth boundary: the radial fill at
@@ -71,4 +79,13 @@ struct gcs_earth {
   void *pool = nullptr;          // geometry of the boundary layers
   void *wind_pool = nullptr;     // monitor time series
   size_t pool_bytes = 0;
+  const gamera_cs_mi_dipole *mi = nullptr;  // coupling named at creation
+  double *mi_pot = nullptr;      // device copy of its potential, 2 x nt x np
+  size_t mi_count = 0;
 };
+
+namespace gcs {
+// Point the device boundary at the MI coupling's current potential (copied
+// to the device) when it is ready; plain wall otherwise.
+int earth_sync_mi(gcs_earth *e, const gamera_cs_mi_dipole *mi);
+}  // namespace gcs

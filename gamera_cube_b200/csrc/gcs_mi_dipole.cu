@@ -32,6 +32,7 @@
 #include "gcs_context.h"
 #include "gcs_error.h"
 #include "gcs_topology.h"
+#include "gcs_mi_lookup.cuh"
 
 using gcs::set_api_error;
 
@@ -240,12 +241,7 @@ double vmag(const gamera_no_vec3 &a) { return sqrt(vdot(a, a)); }
 
 // nonorthogonal_mi.c:168-180
 double mapped_colatitude(double th, double r, double ri) {
-  if (!std::isfinite(th) || !std::isfinite(r) || !std::isfinite(ri) || r <= 0.0 ||
-      ri <= 0.0 || ri > r)
-    return NAN;
-  double arg = sin(th) * sqrt(ri / r);
-  arg = fmax(-1.0, fmin(1.0, arg));
-  return asin(arg);
+  return gcs::mi_mapped_colatitude(th, r, ri);
 }
 
 // nonorthogonal_mi.c:182-195
@@ -268,44 +264,6 @@ bool valid_config(const gamera_cs_mi_dipole_config *c) {
          c->speed_norm_m_s > 0.0 && std::isfinite(c->mass_density_norm_kg_m3) &&
          c->mass_density_norm_kg_m3 > 0.0 && c->maximum_iterations > 0 &&
          std::isfinite(c->relative_tolerance) && c->relative_tolerance > 0.0;
-}
-
-// Earth startup background: dipole (nonorthogonal_background.c:422-442)
-// times the cut ramp (cubedsphere_earth_startup.c:13-19, :87-97).
-int startup_background(const gamera_cs_earth_startup &p, const gamera_no_vec3 &x,
-                       gamera_no_vec3 *out) {
-  const gamera_no_vec3 &m = p.dipole.moment;
-  for (int a = 0; a < 3; ++a)
-    if (!std::isfinite(x.value[a]) || !std::isfinite(m.value[a])) return -1;
-  double r2 = 0.0;
-  for (int a = 0; a < 3; ++a) r2 += x.value[a] * x.value[a];
-  if (!(r2 > DBL_MIN) || !std::isfinite(r2)) return -1;
-  const double r = sqrt(r2);
-  const double ir3 = 1.0 / (r2 * r);
-  const double ir5 = ir3 / r2;
-  double proj = 0.0;
-  for (int a = 0; a < 3; ++a) proj += m.value[a] * x.value[a];
-  for (int a = 0; a < 3; ++a)
-    out->value[a] = 3.0 * proj * ir5 * x.value[a] - ir3 * m.value[a];
-  for (int a = 0; a < 3; ++a)
-    if (!std::isfinite(out->value[a])) return -1;
-  const bool valid = std::isfinite(p.inner_radius) && p.inner_radius > 0.0 &&
-                     std::isfinite(p.density) && p.density > 0.0 &&
-                     std::isfinite(p.speed) && p.speed > 0.0 && std::isfinite(p.mach) &&
-                     p.mach > 0.0 && std::isfinite(p.gamma) && p.gamma > 1.0 &&
-                     std::isfinite(p.ambient_density) && p.ambient_density > 0.0 &&
-                     std::isfinite(p.ambient_pressure) && p.ambient_pressure > 0.0 &&
-                     std::isfinite(p.front_x) && std::isfinite(p.front_width) &&
-                     p.front_width > 0.0 && std::isfinite(p.cut_radius) &&
-                     p.cut_radius > p.inner_radius && std::isfinite(p.cut_length) &&
-                     p.cut_length > 0.0;
-  if (!valid) return -1;
-  const double rr = sqrt(x.value[0] * x.value[0] + x.value[1] * x.value[1] +
-                         x.value[2] * x.value[2]);
-  const double sc = (rr - p.cut_radius) / p.cut_length;
-  const double w = sc <= 0.0 ? 1.0 : (sc >= 1.0 ? 0.0 : 1.0 - 3.0 * sc * sc + 2.0 * sc * sc * sc);
-  for (int a = 0; a < 3; ++a) out->value[a] *= w;
-  return 0;
 }
 
 // Host view of the grid geometry the plans need: the reference-layout grid
@@ -382,6 +340,22 @@ struct gamera_cs_mi_dipole {
 };
 
 namespace {
+
+// Lookup parameters of a coupling with its host copy of the potential.
+gcs::MiLookup lookup_of(const gamera_cs_mi_dipole *s) {
+  gcs::MiLookup L;
+  L.np = s->np;
+  L.nt = s->nt;
+  L.maximum_colatitude = s->maximum_colatitude;
+  L.ionosphere_radius_re = s->config.ionosphere_radius_re;
+  L.length_norm_m = s->config.length_norm_m;
+  L.speed_norm_m_s = s->config.speed_norm_m_s;
+  L.magnetic_norm_t = s->magnetic_norm_t;
+  L.pot[0] = s->pot[0].data();
+  L.pot[1] = s->pot[1].data();
+  L.startup = s->startup;
+  return L;
+}
 
 void destroy_state(gamera_cs_mi_dipole *s) {
   if (!s) return;
@@ -833,6 +807,19 @@ int gamera_cs_mi_dipole_create_potential_view(const gamera_cs_earth_startup *sta
   return 0;
 }
 
+}  // extern "C"
+
+namespace gcs {
+bool mi_lookup(const gamera_cs_mi_dipole *s, MiLookup *L, double *potential_norm_v) {
+  if (s == nullptr || !s->ready) return false;
+  *L = lookup_of(s);
+  *potential_norm_v = s->potential_norm_v;
+  return true;
+}
+}  // namespace gcs
+
+extern "C" {
+
 int gamera_cs_mi_dipole_ready(const gamera_cs_mi_dipole *s) {
   return s != nullptr && s->ready;
 }
@@ -900,31 +887,7 @@ int gamera_cs_mi_dipole_import_potential(gamera_cs_mi_dipole *s, const double *v
 int gamera_cs_mi_dipole_potential(const gamera_cs_mi_dipole *s, gamera_no_vec3 point,
                                   double *potential_v) {
   if (!gamera_cs_mi_dipole_ready(s) || potential_v == nullptr) return -1;
-  const double radius = vmag(point);
-  if (!(radius >= s->config.ionosphere_radius_re)) return -1;
-  const int hemi = point.value[2] >= 0.0 ? 0 : 1;
-  const double th = acos(fmin(1.0, fabs(point.value[2]) / radius));
-  const double thi = mapped_colatitude(th, radius, s->config.ionosphere_radius_re);
-  if (!std::isfinite(thi)) return -1;
-  if (thi >= s->maximum_colatitude) {
-    *potential_v = 0.0;
-    return 0;
-  }
-  const size_t np = (size_t)s->np, nt = (size_t)s->nt;
-  const double tq = thi / s->maximum_colatitude * (double)(nt - 1U);
-  const size_t t = (size_t)floor(tq);
-  const double wt = tq - (double)t;
-  double phi = atan2(point.value[1], point.value[0]);
-  if (phi < 0.0) phi += 2.0 * acos(-1.0);
-  const double pq = phi * (double)np / (2.0 * acos(-1.0));
-  const size_t p = (size_t)floor(pq) % np;
-  const size_t q = (p + 1U) % np;
-  const double wp = pq - floor(pq);
-  const double *pot = s->pot[hemi].data();
-  const double lower = (1.0 - wp) * pot[t * np + p] + wp * pot[t * np + q];
-  const double upper = (1.0 - wp) * pot[(t + 1U) * np + p] + wp * pot[(t + 1U) * np + q];
-  *potential_v = (1.0 - wt) * lower + wt * upper;
-  return std::isfinite(*potential_v) ? 0 : -1;
+  return gcs::mi_potential(lookup_of(s), point, potential_v);
 }
 
 // cubedsphere_mi_dipole.c:478-503
@@ -957,39 +920,7 @@ int gamera_cs_mi_dipole_ghost_velocity(const gamera_cs_mi_dipole *s, gamera_no_v
                                        gamera_no_vec3 source_velocity,
                                        gamera_no_vec3 *ghost_velocity) {
   if (!gamera_cs_mi_dipole_ready(s) || ghost_velocity == nullptr) return -1;
-  const double radius = vmag(point);
-  if (!(radius > 0.0)) return -1;
-  const double eps = 1e-4 * fmax(1.0, radius);
-  gamera_no_vec3 e = {{0.0, 0.0, 0.0}};
-  for (int c = 0; c < 3; ++c) {
-    gamera_no_vec3 plus = point, minus = point;
-    plus.value[c] += eps;
-    minus.value[c] -= eps;
-    double pp, pm;
-    if (gamera_cs_mi_dipole_potential(s, plus, &pp) != 0 ||
-        gamera_cs_mi_dipole_potential(s, minus, &pm) != 0)
-      return -1;
-    e.value[c] = -(pp - pm) / (2.0 * eps * s->config.length_norm_m *
-                               s->config.speed_norm_m_s * s->magnetic_norm_t);
-  }
-  gamera_no_vec3 bg;
-  if (startup_background(s->startup, point, &bg) != 0) return -1;
-  const double b2 = vdot(bg, bg);
-  if (!(b2 > 0.0)) return -1;
-  gamera_no_vec3 drift = {{(e.value[1] * bg.value[2] - e.value[2] * bg.value[1]) / b2,
-                           (e.value[2] * bg.value[0] - e.value[0] * bg.value[2]) / b2,
-                           (e.value[0] * bg.value[1] - e.value[1] * bg.value[0]) / b2}};
-  const double radial = vdot(drift, point) / (radius * radius);
-  for (int c = 0; c < 3; ++c) drift.value[c] -= radial * point.value[c];
-  // gamera_mi_compose_ghost_velocity
-  double bsq = 0.0;
-  for (int c = 0; c < 3; ++c) bsq += bg.value[c] * bg.value[c];
-  if (!(bsq > 0.0) || !std::isfinite(bsq)) return -1;
-  for (int c = 0; c < 3; ++c) {
-    ghost_velocity->value[c] = 2.0 * drift.value[c] - source_velocity.value[c];
-    if (!std::isfinite(ghost_velocity->value[c])) return -1;
-  }
-  return 0;
+  return gcs::mi_ghost_velocity(lookup_of(s), point, source_velocity, ghost_velocity);
 }
 
 // cubedsphere_mi_dipole.c:545-570

@@ -385,9 +385,10 @@ int gcs_context_bulk_split(const gcs_context *ctx);
  * gamera_cs_earth_fill_radial_ghosts with options->fluid_flux_sync =
  * gamera_cs_earth_inner_fluid_flux, options->edge_emf_sync =
  * gamera_cs_earth_no_mi_emf and the same boundary as both contexts), they
- * run as device kernels inside the step with no host round trip unless the
- * boundary's MI coupling is ready; called directly they work on host
- * storage (the radial fill through the grid's device context). */
+ * run as device kernels inside the step with no host round trip, a ready
+ * MI coupling included (its potential copied to the device each step);
+ * called directly they work on host storage (the radial fill through the
+ * grid's device context). */
 int gamera_cs_earth_fill_radial_ghosts(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
                                        gamera_no_storage storage[GAMERA_CS_FACE_COUNT],
                                        const size_t active[3], size_t ghost,
@@ -412,8 +413,9 @@ int gamera_cs_earth_no_mi_emf(gamera_no_storage *storage, const gamera_no_grid *
  * (:298-451) as kernels at the reference step's callback positions.
  * gcs_earth_create copies the boundary layers' geometry from `grid`, the
  * outer faces' B0 flux from boundary->background and the monitor series
- * boundary->wind to the device; an MI-coupled wall (boundary->mi ready)
- * is refused: it stays on the host callback path. */
+ * boundary->wind to the device; with boundary->mi set, each step uses its
+ * potential while it is ready (MI-coupled wall: E x B drift ghost velocity,
+ * inner-shell EMF from the potential). */
 typedef struct gcs_earth gcs_earth;
 int gcs_earth_create(gcs_context *ctx, const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
                      const gamera_cs_earth_boundary *boundary, gcs_earth **earth);

@@ -311,3 +311,93 @@ def test_device_built_case_boundary_matches_host_grid(lib):
         for ctx in (a, d):
             if ctx:
                 lib.gcs_context_destroy(ctx)
+
+
+@pytest.mark.parametrize("strict", [0, 1])
+def test_drop_in_step_with_mi_coupled_wall(lib, strict):
+    """The Earth step with a ready MI coupling (potential views of both
+    libraries holding the reference's solved potential of the coupling
+    test): E x B drift ghost velocities and the inner-shell EMF from the
+    potential, on the device, against the reference's host callbacks.
+    Tolerance 1e-10: the drift is a central difference of the mapped
+    potential over 1e-4 R_E, which turns the last-bit differences of the
+    device's acos/asin/atan2 in the lookup into ~1e-12 relative in E."""
+    if not refbind.ref_available():
+        pytest.skip("reference library not built")
+    import mi_util
+    R = refbind.ref()
+    abi.bind(R, abi.earth_callback_signatures())
+    abi.bind(R, {"gamera_cs_mi_dipole_create_potential_view":
+                 (C.c_int, [C.POINTER(abi.EarthStartup), C.POINTER(abi.MiDipoleConfig),
+                            C.POINTER(C.c_void_p)])})
+    cfg, startup = mi_util.coupling_config(), mi_util.coupling_startup()
+    pot = np.ascontiguousarray(mi_util.golden()["coupling/potential"])
+    P = C.POINTER(C.c_double)
+    views = []
+    for L in (R, lib):
+        mi = C.c_void_p()
+        assert L.gamera_cs_mi_dipole_create_potential_view(C.byref(startup), C.byref(cfg),
+                                                           C.byref(mi)) == 0
+        assert L.gamera_cs_mi_dipole_import_potential(mi, pot.ctypes.data_as(P), pot.size,
+                                                      0.0, 10.0) == 0
+        views.append(mi)
+    ref = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    gpu = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+    keep = []
+    wind = wind_series(keep)
+    b_ref = boundary(startup, wind, ref.background, strict)
+    b_gpu = boundary(startup, wind, gpu.background, strict)
+    b_ref.mi, b_gpu.mi = views[0].value, views[1].value
+    ropts, gopts = earth_options(R, ref, b_ref), earth_options(lib, gpu, b_gpu)
+    plan = C.c_void_p()
+    assert lib.gamera_cs_halo_plan_create(gpu.grid, gpu.active, gpu.ghost, C.byref(plan)) == 0
+    try:
+        time, dt_prev = 0.0, 0.0
+        for s in range(3):
+            local = ref.local_timestep()
+            dt = 0.5 * local if dt_prev == 0.0 else min(0.5 * local, 1.25 * dt_prev)
+            ratio = 0.0 if dt_prev == 0.0 else 0.5 * dt / dt_prev
+            prev = time if s == 0 else time - dt_prev
+            for bd in (b_ref, b_gpu):
+                bd.step_time, bd.step_dt = time, dt
+            assert R.gamera_cs_advance_six_with_background_planned(
+                ref.grid, ref.storage, ref.active, ref.ghost, ratio, dt, C.byref(ropts),
+                ref.background, R.fx_plan(ref.handle),
+                C.cast(R.gamera_cs_earth_fill_radial_ghosts, C.c_void_p),
+                time, prev, C.cast(C.pointer(b_ref), C.c_void_p)) == 0
+            assert lib.gamera_cs_advance_six_with_background_planned(
+                gpu.grid, gpu.storage, gpu.active, gpu.ghost, ratio, dt, C.byref(gopts),
+                gpu.background, plan, C.cast(lib.gamera_cs_earth_fill_radial_ghosts,
+                                             C.c_void_p),
+                time, prev, C.cast(C.pointer(b_gpu), C.c_void_p)) == 0
+            res = compare_state(gpu, ref, NAMES)
+            bad = {k: v for k, v in res.items() if not v[0] <= 1e-10 * 10 ** s}
+            assert not bad, "step %d: %s" % (s, bad)
+            time += dt
+            dt_prev = dt
+        # the MI wall acted: one reference step without the coupling differs
+        plain = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+        b_plain = boundary(startup, wind, plain.background, strict)
+        po = earth_options(R, plain, b_plain)
+        once = refbind.Case(refbind.FX_WIND, 12, 10, 7)
+        b_once = boundary(startup, wind, once.background, strict)
+        b_once.mi = views[0].value
+        oo = earth_options(R, once, b_once)
+        dt = 0.5 * plain.local_timestep()
+        for case, bd, o in ((plain, b_plain, po), (once, b_once, oo)):
+            bd.step_time, bd.step_dt = 0.0, dt
+            assert R.gamera_cs_advance_six_with_background_planned(
+                case.grid, case.storage, case.active, case.ghost, 0.0, dt, C.byref(o),
+                case.background, R.fx_plan(case.handle),
+                C.cast(R.gamera_cs_earth_fill_radial_ghosts, C.c_void_p), 0.0, 0.0,
+                C.cast(C.pointer(bd), C.c_void_p)) == 0
+        assert any(not np.array_equal(plain.arrays(f)["edge_emf1"], once.arrays(f)["edge_emf1"])
+                   for f in range(6))
+        plain.close()
+        once.close()
+    finally:
+        lib.gamera_cs_halo_plan_destroy(plan)
+        R.gamera_cs_mi_dipole_destroy(views[0])
+        lib.gamera_cs_mi_dipole_destroy(views[1])
+        ref.close()
+        gpu.close()

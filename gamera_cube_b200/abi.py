@@ -293,6 +293,14 @@ def ensemble_signatures():
                                              C.c_double]),
     }
     sig.update(earth_callback_signatures())
+    sig.update({
+        "gcs_analysis_frame_floats": (C.c_size_t, [C.c_void_p]),
+        "gcs_context_analysis_frame": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p,
+                                                 C.c_void_p]),
+        "gcs_context_write_analysis": (C.c_int, [C.c_void_p, C.c_char_p, C.c_long, C.c_long,
+                                                 C.c_double, C.c_double, C.c_double,
+                                                 P(Grid)]),
+    })
     return sig
 
 

@@ -784,6 +784,7 @@ int Context::init_case(int kind, size_t nr, size_t n, unsigned long long seed,
     return -1;
   }
   const WindInit wi = driver ? *driver : case_wind(kind);
+  kind_shock = kind == 1;
   const int wind = kind >= 2;
   const size_t active[3] = {nr, n, n};
   if (allocate(active, 4) != 0) return -1;
@@ -987,6 +988,71 @@ int Context::init_member(Context &o, unsigned long long seed, const WindInit &w)
     set_error("degenerate geometry or invalid initial state", "init_member");
     return -1;
   }
+  return 0;
+}
+
+__global__ void k_active_centroids(Dims D, const gamera_no_cell_geometry *cells, double *out) {
+  const long long count = (long long)D.nr * D.n * D.n;
+  const long long t = tid();
+  if (t >= count) return;
+  const int i = (int)(t / ((long long)D.n * D.n));
+  const int j = (int)((t / D.n) % D.n);
+  const int k = (int)(t % D.n);
+  const gamera_no_vec3 x =
+      cells[((long long)(i + D.g) * D.E1 + j + D.g) * D.E2 + k + D.g].centroid;
+  for (int a = 0; a < 3; ++a) out[a * count + t] = x.value[a];
+}
+
+__global__ void k_active_vertices(Dims D, const V3 *vert, double *out) {
+  const long long count = (long long)(D.nr + 1) * (D.n + 1) * (D.n + 1);
+  const long long t = tid();
+  if (t >= count) return;
+  const int i = (int)(t / ((long long)(D.n + 1) * (D.n + 1)));
+  const int j = (int)((t / (D.n + 1)) % (D.n + 1));
+  const int k = (int)(t % (D.n + 1));
+  const V3 x = vert[((long long)(i + D.g) * (D.E1 + 1) + j + D.g) * (D.E2 + 1) + k + D.g];
+  out[t] = x.x;
+  out[count + t] = x.y;
+  out[2 * count + t] = x.z;
+}
+
+// Active-cell centroids [3][nr][n][n] and active vertices
+// [3][nr+1][n+1][n+1] of one face of a device-built case, rebuilt on the
+// device (analysis grid output).
+int Context::face_coordinates(int f, std::vector<double> &cen, std::vector<double> &vert_out) {
+  if (owner || !staging || grid_cell[0] != nullptr || f < 0 || f >= kFaces) {
+    set_error("needs a device-built case", "face_coordinates");
+    return -1;
+  }
+  const Dims &D = X.D;
+  const long long cells = (long long)D.E0 * D.E1 * D.E2;
+  const long long verts = (long long)(D.E0 + 1) * (D.E1 + 1) * (D.E2 + 1);
+  const long long nc = (long long)D.nr * D.n * D.n;
+  const long long nv = (long long)(D.nr + 1) * (D.n + 1) * (D.n + 1);
+  void *work = nullptr;
+  GCS_BTRY(cudaMalloc(&work, verts * sizeof(V3) + 3 * (nc + nv) * sizeof(double) + sizeof(int)));
+  V3 *vert = (V3 *)work;
+  double *dc = (double *)(vert + verts);
+  double *dv = dc + 3 * nc;
+  int *bad = (int *)(dv + 3 * nv);
+  const int wind = bg_pool != nullptr;
+  const double r_in = wind ? 2.5 : 2.0;
+  const double r_out = wind ? 30.0 : (kind_shock ? 3.0 : 2.5);
+  const int bs = 128;
+  k_vertices<<<nblk(verts, bs), bs, 0, stream>>>(f, D.nr, D.n, D.g, r_in, r_out,
+                                                 wind ? log(12.0) : 0.0, vert);
+  k_cells<<<nblk(cells, 64), 64, 0, stream>>>(D, vert, (gamera_no_cell_geometry *)staging, bad);
+  k_active_centroids<<<nblk(nc, bs), bs, 0, stream>>>(D, (gamera_no_cell_geometry *)staging, dc);
+  k_active_vertices<<<nblk(nv, bs), bs, 0, stream>>>(D, vert, dv);
+  cen.resize(3 * nc);
+  vert_out.resize(3 * nv);
+  GCS_BTRY(cudaGetLastError());
+  GCS_BTRY(cudaMemcpyAsync(cen.data(), dc, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost,
+                           stream));
+  GCS_BTRY(cudaMemcpyAsync(vert_out.data(), dv, 3 * nv * sizeof(double),
+                           cudaMemcpyDeviceToHost, stream));
+  GCS_BTRY(cudaStreamSynchronize(stream));
+  cudaFree(work);
   return 0;
 }
 

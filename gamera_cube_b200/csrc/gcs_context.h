@@ -65,6 +65,10 @@ struct Context {
   // (gcs_build.cu); no host grid is involved.
   int init_case(int kind, size_t nr, size_t n, unsigned long long seed,
                 const WindInit *driver = nullptr);
+  // Active centroids and vertices of one face of a device-built case
+  // (gcs_build.cu).
+  int face_coordinates(int f, std::vector<double> &centroids, std::vector<double> &vertices);
+  int kind_shock = 0;   // device-built radial shock case (r in [2, 3])
   // Radial boundary-layer geometry of a device-built wind case for the
   // device Earth boundary (gcs_build.cu).
   int build_earth_layers(const EarthLayers &L);

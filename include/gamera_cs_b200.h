@@ -448,6 +448,27 @@ int gcs_context_step_earth(gcs_context *ctx, gcs_earth *earth,
                            double predictor_ratio, double dt, double current_time,
                            double previous_time);
 
+/* Analysis output (cubedsphere/cubedsphere_analysis_hdf5.c:299-355,
+ * cubedsphere/docs/OUTPUT_DATA_MODEL.md).  The frame of a face is float32
+ * [8][nr][n][n]: rho, p, vx, vy, vz (primitives with floors 1e-12 and the
+ * given gamma) and Bx, By, Bz (residual plus cell B0 where the context has a
+ * background) over the active cells; six faces in order.  Computed on the
+ * device into `device_out` (gcs_analysis_frame_floats floats) and/or
+ * copied to `host_out`.  Fails on an invalid state or a non-finite field,
+ * as the reference writer does. */
+size_t gcs_analysis_frame_floats(const gcs_context *ctx);
+int gcs_context_analysis_frame(gcs_context *ctx, double gamma, float *device_out,
+                               float *host_out);
+/* The reference's per-face file set in `directory` with raw little-endian
+ * datasets and JSON metadata in place of HDF5: analysis_grid_p<f>.json with
+ * .coordinates.f64 [3][nr][n][n] and .vertices.f64 [3][nr+1][n+1][n+1]
+ * (written when absent; from `grid`, or rebuilt on the device for a
+ * device-built case when grid is NULL), and analysis_p<f>_<sequence:06>.json
+ * with .state.f32 (the frame) and the reference's metadata datasets. */
+int gcs_context_write_analysis(gcs_context *ctx, const char *directory, long sequence,
+                               long step, double time_code, double time_seconds,
+                               double gamma, const gamera_no_grid *grid);
+
 /* Upstream solar wind of a wind run (no reference counterpart; the
  * reference driver fixes it at n = 5 cm^-3, V = -400 km/s, T = 1e5 K,
  * Bz = -5 nT, test_cubedsphere_dipole_background.c:282-294): density

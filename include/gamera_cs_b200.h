@@ -491,7 +491,7 @@ gcs_context *gcs_context_create_wind(size_t nr, size_t n, unsigned long long see
  * is a tile of bx consecutive points of the flattened (j, k) plane of a
  * radial layer times by radial layers; bx * by must be a multiple of 32 and
  * at most gcs_tile_limit(family).  Tiles change speed, never results.
- * Defaults: 128 x 1 (recovery/CFL 256 x 1). */
+ * Defaults: 64 x 1 for the flux and edge-EMF sweeps, 128 x 1 otherwise. */
 enum {
   GCS_TILE_PREDICT = 0,
   GCS_TILE_FLUX = 1,

@@ -201,9 +201,9 @@ def test_ensemble_runs_equal_standalone_runs(lib, bulk):
             finally:
                 lib.gcs_context_destroy(alone)
         # runs with different drivers differ
-        s0 = download(lib, lib.gcs_ensemble_run_context(e, 0)).arrays(0)["conserved"]
-        s2 = download(lib, lib.gcs_ensemble_run_context(e, 2)).arrays(0)["conserved"]
-        assert not np.array_equal(s0, s2)
+        h0 = download(lib, lib.gcs_ensemble_run_context(e, 0))
+        h2 = download(lib, lib.gcs_ensemble_run_context(e, 2))
+        assert not np.array_equal(h0.arrays(0)["conserved"], h2.arrays(0)["conserved"])
     finally:
         lib.gcs_ensemble_destroy(e)
 

@@ -291,7 +291,7 @@ __global__ void k_face_velocity(Dims D, Bulk<T> B, DevStatus *st, int i0,
 // ---------------------------------------------------------------------------
 // Edge EMF sweep of edge family e (nonorthogonal_sweep.c:624-752).
 template <int e, typename T>
-__global__ void __launch_bounds__(128) k_edge_emf(Dims D, DevState S, DevGeom G,
+__global__ void __launch_bounds__(128, 5) k_edge_emf(Dims D, DevState S, DevGeom G,
                                                   Bulk<T> B, Opts O,
                                                   const StepParams *prm,
                                                   DevStatus *st, int i0,
@@ -427,7 +427,7 @@ __global__ void k_ct(Dims D, DevState S, Opts O, const StepParams *prm, DevStatu
 // nonorthogonal_sweep.c:550-622): save U, B as old on every cell, then on
 // active cells U += dt * rate, recover B from the CT-updated Phi, and apply
 // the Boris (nonorthogonal_state.c:161-280) or Maxwell momentum update.
-__global__ void __launch_bounds__(128) k_update(Dims D, DevState S, DevGeom G,
+__global__ void __launch_bounds__(128, 6) k_update(Dims D, DevState S, DevGeom G,
                                                 DevBg BG, Opts O,
                                                 const StepParams *prm,
                                                 DevStatus *st) {

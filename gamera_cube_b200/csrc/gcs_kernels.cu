@@ -429,19 +429,19 @@ static int bulk_split(const Ctx &X) { return X.bulk ? X.bulk_split : X.D.E0 + 1;
 
 void launch_flux(const Ctx &X, const Opts &O, cudaStream_t s) {
   const int sp = bulk_split(X);
-  Sweeps<double>::flux(X, bulk64(X), O, 0, sp, s);
+  launch_flux_f64(X, O, 0, sp, s);
   if (X.bulk) launch_flux_f32(X, O, sp, X.D.E0 + 1, s);
 }
 
 void launch_face_velocities(const Ctx &X, const Opts &O, cudaStream_t s) {
   const int sp = bulk_split(X);
-  Sweeps<double>::emf(X, bulk64(X), O, 0, sp, s);
+  launch_face_velocity_f64(X, O, 0, sp, s);
   if (X.bulk) launch_face_velocity_f32(X, O, sp, X.D.E0 + 1, s);
 }
 
 void launch_edge_emfs(const Ctx &X, const Opts &O, cudaStream_t s) {
   const int sp = bulk_split(X);
-  Sweeps<double>::edge(X, bulk64(X), O, 0, sp, s);
+  launch_edge_emf_f64(X, O, 0, sp, s);
   if (X.bulk) launch_edge_emf_f32(X, O, sp, X.D.E0 + 1, s);
 }
 

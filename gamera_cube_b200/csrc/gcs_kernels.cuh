@@ -54,6 +54,12 @@ inline dim3 tile_block(Tile t) { return dim3((unsigned)t.bx, (unsigned)t.by, 1);
 // Bulk<double> view of the FP64 arrays.
 Bulk<double> bulk64(const Ctx &X);
 
+// FP64 sweeps over the radial range [i0, i1) (gcs_kernels_fp64.cu).
+void launch_flux_f64(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s);
+void launch_face_velocity_f64(const Ctx &X, const Opts &O, int i0, int i1,
+                              cudaStream_t s);
+void launch_edge_emf_f64(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s);
+
 // FP32-bulk sweeps over the radial range [i0, i1) (gcs_kernels_bulk.cu).
 void launch_flux_f32(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s);
 void launch_face_velocity_f32(const Ctx &X, const Opts &O, int i0, int i1,

@@ -40,7 +40,7 @@ NR, N = 192, 96                 # active radial, angular cells per face
 KIND_WIND = 2
 METRIC = "MHD cell-updates/s on 1 B200 (FP64 plain path)"
 # Algorithmic bytes per cell-update of the whole step (state 192 B +
-# compacted metric 664 B + background 192 B; see DESIGN.md).
+# compacted metric 664 B + background 192 B).
 STEP_BYTES_PER_CELL = 1048
 # Per-launch algorithmic bytes per face of the flux sweep: cells U~ (5),
 # B~ (3), volume (1) counted once per face along the sweep, face Phi~ (1),
@@ -149,8 +149,11 @@ def sum_over_ranks(value, dist, device):
 def barrier(dist, device):
     if dist is not None:
         import torch
-        dist.barrier(device_ids=[device.index])
-        torch.cuda.synchronize(device)
+        if device.type == "cuda":
+            dist.barrier(device_ids=[device.index])
+            torch.cuda.synchronize(device)
+        else:
+            dist.barrier()
 
 
 def run_gpu(args):

@@ -15,6 +15,14 @@
 // sweep launch covers one radial range [i0, i1).
 #pragma once
 
+#ifndef GCS_F32_FLUX_BLOCKS
+#define GCS_F32_FLUX_BLOCKS 8
+#endif
+#ifndef GCS_F32_EDGE_BLOCKS
+#define GCS_F32_EDGE_BLOCKS 8
+#endif
+
+
 #include "gcs_kernel_util.cuh"
 #include "gcs_kernels.cuh"
 #include "gcs_physics.cuh"
@@ -100,13 +108,27 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
 }
 #endif  // GCS_SWEEPS_TEMPLATES_ONLY
 
+// Minimum resident blocks of 128 threads per SM the sweeps are compiled for
+// (register caps 128 and 96 in FP64, 64 in FP32), from measured full-step
+// sweeps at 6 x 96x96x192.
+template <typename T>
+struct SweepOccupancy {
+  static constexpr int flux = 4;
+  static constexpr int edge = 5;
+};
+template <>
+struct SweepOccupancy<float> {
+  static constexpr int flux = GCS_F32_FLUX_BLOCKS;
+  static constexpr int edge = GCS_F32_EDGE_BLOCKS;
+};
+
 // ---------------------------------------------------------------------------
 // Face-flux sweep in direction d (nonorthogonal_sweep.c:408-548).
 // Each thread owns one face; the eight-cell stencil of one variable at a
 // time is read from the predictor's cell primitives, so only the volumes,
 // one stencil and the reconstructed face states are live at once.
 template <int d, typename T>
-__global__ void __launch_bounds__(128, 4) k_flux(Dims D, DevState S, Bulk<T> B,
+__global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, DevState S, Bulk<T> B,
                                                  Opts O, DevStatus *st, int i0,
                                                  int i1) {
   if (failed(st)) return;
@@ -291,7 +313,7 @@ __global__ void k_face_velocity(Dims D, Bulk<T> B, DevStatus *st, int i0,
 // ---------------------------------------------------------------------------
 // Edge EMF sweep of edge family e (nonorthogonal_sweep.c:624-752).
 template <int e, typename T>
-__global__ void __launch_bounds__(128, 5) k_edge_emf(Dims D, DevState S, DevGeom G,
+__global__ void __launch_bounds__(128, SweepOccupancy<T>::edge) k_edge_emf(Dims D, DevState S, DevGeom G,
                                                   Bulk<T> B, Opts O,
                                                   const StepParams *prm,
                                                   DevStatus *st, int i0,

@@ -410,8 +410,9 @@ def run_bulk(lib, torch, device, args, dist):
 def run_earth(lib, torch, device, args, dist, ctx):
     """The production case stepped with the device Earth radial boundary
     (no-MI wall): radial ghosts from a constant upstream monitor (the case's
-    own wind), inner flux trap, wind-driven outer EMF, one
-    gcs_context_step_earth call per step (host-driven dt, no graph)."""
+    own wind), inner flux trap, wind-driven outer EMF, in the device driver
+    loop (gcs_context_run_earth: dt and times on the device, one CUDA graph
+    per step)."""
     from gamera_cube_b200 import abi
     opts, ts = abi.AdvanceOptions(), abi.TimestepOptions()
     lib.gcs_case_options(KIND_WIND, C.byref(opts), C.byref(ts))
@@ -435,28 +436,19 @@ def run_earth(lib, torch, device, args, dist, ctx):
     if lib.gcs_earth_create_case(ctx, C.byref(b), C.byref(earth)) != 0:
         return {"error": lib.gcs_last_error().decode()}
     stream = torch.cuda.ExternalStream(lib.gcs_context_stream(ctx), device=device)
-    local = C.c_double()
-    lib.gcs_context_timestep(ctx, C.byref(ts), C.byref(local))
-    dt = 0.5 * local.value
-    clock = [0.0]
-
-    def steps(k):
-        for _ in range(k):
-            prev = clock[0] - dt if clock[0] > 0.0 else clock[0]
-            if lib.gcs_context_step_earth(ctx, earth, C.byref(opts), 0.5 if clock[0] > 0 else 0.0,
-                                          dt, clock[0], prev) != 0:
-                return False
-            clock[0] += dt
-        return True
-
-    ok = steps(3)
+    # driver mode: dt, predictor ratio and the boundary's times on the device,
+    # one CUDA graph per step
+    ok = lib.gcs_context_run_earth(ctx, earth, C.byref(opts), C.byref(ts), 0.5, 3, 1) == 0
+    ok = ok and lib.gcs_context_sync(ctx) == 0
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(dist, device)
     torch.cuda.synchronize()
     start.record(stream)
-    ok = ok and steps(args.earth_steps)
+    ok = ok and lib.gcs_context_run_earth(ctx, earth, C.byref(opts), C.byref(ts), 0.5,
+                                          args.earth_steps, 1) == 0
     stop.record(stream)
     stop.synchronize()
+    ok = ok and lib.gcs_context_sync(ctx) == 0
     ms = max_over_ranks(start.elapsed_time(stop), dist, device)
     act = (C.c_size_t * 3)()
     g = C.c_size_t()
@@ -469,9 +461,9 @@ def run_earth(lib, torch, device, args, dist, ctx):
             "ms_per_step": ms / args.earth_steps, "steps": args.earth_steps, "ok": bool(ok),
             "workload": "6 x %dx%dx%d wind + dipole, device Earth radial boundary (no-MI wall), "
                         "constant upstream monitor" % (act[1], act[2], act[0]),
-            "call": "gcs_context_step_earth (host-driven step, status read back each step)",
+            "call": "gcs_context_run_earth (device driver loop, one CUDA graph per step)",
             "boundary_device_bytes": nbytes,
-            "gpu_launches_per_step": 22 + 19}
+            "gpu_launches_per_step": 24 + 19}
 
 
 ENS_SEED = 2024

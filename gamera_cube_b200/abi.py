@@ -291,6 +291,9 @@ def ensemble_signatures():
         "gcs_context_step_earth": (C.c_int, [C.c_void_p, C.c_void_p, P(AdvanceOptions),
                                              C.c_double, C.c_double, C.c_double,
                                              C.c_double]),
+        "gcs_context_run_earth": (C.c_int, [C.c_void_p, C.c_void_p, P(AdvanceOptions),
+                                            P(TimestepOptions), C.c_double, C.c_int,
+                                            C.c_int]),
     }
     sig.update(earth_callback_signatures())
     sig.update({

@@ -233,7 +233,7 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   gcs::launch_seam_sync(X, 1, s);
   mk.mark(kSlotSeamPhi);
   gcs::launch_halo(X, s);
-  if (es) gcs::launch_earth_radial(X, *es->dev, es->current_time, es->previous_time, s);
+  if (es) gcs::launch_earth_radial(X, *es, s);
   mk.mark(kSlotHalo);
   const size_t lower[3] = {hk ? hk->ghost : 0, hk ? hk->ghost : 0,
                            hk ? hk->ghost : 0};
@@ -265,7 +265,7 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   }
   if (O.u_mhd) {
     gcs::launch_emf(X, O, s);
-    if (es) gcs::launch_earth_emf(X, *es->dev, es->step_time, es->step_dt, s);
+    if (es) gcs::launch_earth_emf(X, *es, s);
     mk.mark(kSlotEmf);
     if (hk && hk->options->edge_emf_sync) {
       if (device_failed(C) || transfer_emf(C, hk->storage, false) != 0)
@@ -405,7 +405,7 @@ int drop_in_step(gcs_context *ctx, const gamera_no_grid grid[6],
     if (!std::isfinite(eb->step_time) || !(eb->step_dt > 0.0)) return -1;
     gcs_earth *earth = gcs::earth_for(C, grid, eb, true);
     if (earth == nullptr) return -1;
-    const gcs::EarthStep es{&earth->dev, t, tprev, eb->step_time, eb->step_dt};
+    const gcs::EarthStep es{&earth->dev, t, tprev, eb->step_time, eb->step_dt, 0};
     rc = run_step(ctx, O, 0, nullptr, &es);
   } else {
     Hooks hk{grid, storage, active, ghost, radial, t, tprev, radial_ctx, options};
@@ -994,7 +994,7 @@ int gcs_context_step_earth(gcs_context *ctx, gcs_earth *earth,
   if (gcs::earth_sync_mi(earth, earth->mi) != 0) return -1;
   // the reference driver sets step_time = current time, step_dt = dt
   // (test_cubedsphere_dipole_background.c:667-668)
-  const gcs::EarthStep es{&earth->dev, current_time, previous_time, current_time, dt};
+  const gcs::EarthStep es{&earth->dev, current_time, previous_time, current_time, dt, 0};
   const int rc = run_step(ctx, O, 0, nullptr, &es);
   const bool fail = device_failed(C);
   if (fail) report_failure(C);
@@ -1018,9 +1018,15 @@ int gcs_context_timestep(gcs_context *ctx, const gamera_no_timestep_options *t,
   return 0;
 }
 
-int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
-                    const gamera_no_timestep_options *t, double fraction,
-                    int steps, int use_graph) {
+}  // extern "C"
+
+namespace {
+
+// The driver loop of gcs_context_run, optionally with the device Earth
+// boundary in driver mode (times from the step parameters).
+int context_run(gcs_context *ctx, const gamera_no_advance_options *options,
+                const gamera_no_timestep_options *t, double fraction, int steps,
+                int use_graph, const gcs::EarthStep *es) {
   if (!ctx || steps < 0 || !std::isfinite(fraction) || fraction <= 0.0) return -1;
   gcs::Opts O;
   if (!make_opts(options, ctx->c.bg_uploaded != 0, &O) ||
@@ -1050,6 +1056,11 @@ int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
     const unsigned char *b = (const unsigned char *)&O;
     for (size_t q = 0; q < sizeof(O); ++q) key = (key ^ b[q]) * 1099511628211ULL;
     key = (key ^ (unsigned long long)C.X.bulk) * 1099511628211ULL;
+    if (es) {
+      const unsigned char *e = (const unsigned char *)es->dev;
+      for (size_t q = 0; q < sizeof(*es->dev); ++q) key = (key ^ e[q]) * 1099511628211ULL;
+      key = (key ^ 0x45415254ULL) * 1099511628211ULL;
+    }
     for (int f = 0; f < gcs::kTileFamilies; ++f)
       key = (key ^ (unsigned long long)(C.X.tile[f].bx * 64 + C.X.tile[f].by)) *
             1099511628211ULL;
@@ -1060,7 +1071,7 @@ int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
       if (cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal) !=
           cudaSuccess)
         return -1;
-      run_step(ctx, O, 1, nullptr);
+      run_step(ctx, O, 1, nullptr, es);
       if (cudaStreamEndCapture(C.stream, &graph) != cudaSuccess) return -1;
       const cudaError_t ie = cudaGraphInstantiate(&C.graph_exec, graph, 0);
       cudaGraphDestroy(graph);
@@ -1071,9 +1082,29 @@ int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
       if (cudaGraphLaunch(C.graph_exec, C.stream) != cudaSuccess) return -1;
   } else {
     for (int q = 0; q < steps; ++q)
-      if (run_step(ctx, O, 1, nullptr) != 0) return -1;
+      if (run_step(ctx, O, 1, nullptr, es) != 0) return -1;
   }
   return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
+                    const gamera_no_timestep_options *t, double fraction,
+                    int steps, int use_graph) {
+  return context_run(ctx, options, t, fraction, steps, use_graph, nullptr);
+}
+
+int gcs_context_run_earth(gcs_context *ctx, gcs_earth *earth,
+                          const gamera_no_advance_options *options,
+                          const gamera_no_timestep_options *t, double fraction,
+                          int steps, int use_graph) {
+  if (!ctx || !earth || earth->C != &ctx->c) return -1;
+  if (gcs::earth_sync_mi(earth, earth->mi) != 0) return -1;
+  const gcs::EarthStep es{&earth->dev, 0.0, 0.0, 0.0, 0.0, 1};
+  return context_run(ctx, options, t, fraction, steps, use_graph, &es);
 }
 
 int gcs_context_sync(gcs_context *ctx) {

@@ -119,6 +119,7 @@ struct StepParams {
   double cfl_min;       // min CFL step of the state after the last step
   int step;             // number of completed steps
   int pad;
+  double time;          // simulation time of the state (driver mode)
 };
 
 // Physics options of one call, one group per reference option struct:

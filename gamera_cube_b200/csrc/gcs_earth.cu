@@ -138,6 +138,13 @@ __host__ __device__ inline bool sample_wind(const WindDev &w, const double x[3],
   return wind_sample_at(w, x, t, s) && wind_weight(x, *s, weight);
 }
 
+// Times of a launch: the host's values, or the driver-mode values in the
+// step parameters (prm non-null).
+__device__ inline double radial_time(const StepParams *prm, double time, int old) {
+  if (prm == nullptr) return time;
+  return old && prm->step > 0 ? prm->time - prm->dt_prev : prm->time;
+}
+
 __device__ inline long long plane(const Dims &D, int f, int layers, int l, int j, int k) {
   return (((long long)f * layers + l) * D.N1 + j) * D.N2 + k;
 }
@@ -148,8 +155,9 @@ __device__ inline long long plane(const Dims &D, int f, int layers, int l, int j
 // wall); outer ghosts take the last active cell, raise a subsonic outward
 // velocity to the sound speed and blend with the sampled wind.
 __global__ void k_earth_cells(Dims D, DevState S, EarthDev E, double time, int old,
-                              DevStatus *st) {
+                              const StepParams *prm, DevStatus *st) {
   if (failed(st)) return;
+  time = radial_time(prm, time, old);
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
   if (jk >= D.E1 * D.E2) return;
   const int l = blockIdx.y, f = blockIdx.z;
@@ -226,8 +234,9 @@ __global__ void k_earth_cells(Dims D, DevState S, EarthDev E, double time, int o
 // blend the wind's residual flux (B_wind . area vector - B0 flux) with the
 // last face inside.
 __global__ void k_earth_faces(Dims D, DevState S, DevGeom G, EarthDev E, int d,
-                              double time, int old, DevStatus *st) {
+                              double time, int old, const StepParams *prm, DevStatus *st) {
   if (failed(st)) return;
+  time = radial_time(prm, time, old);
   const int e1 = D.E1 + (d == 1), e2 = D.E2 + (d == 2);
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
   if (jk >= e1 * e2) return;
@@ -318,8 +327,9 @@ __global__ void k_earth_trap(Dims D, DevState S) {
 // blend the EMF with the wind's -v x B line integral, the weight falling as
 // 1 / (1 + layers inside), cubedsphere_earth_boundary.c:390-425.
 __global__ void k_earth_emf_outer(Dims D, DevState S, EarthDev E, int d, double tmid,
-                                  DevStatus *st) {
+                                  const StepParams *prm, DevStatus *st) {
   if (failed(st)) return;
+  if (prm) tmid = prm->time + 0.5 * prm->dt;
   const int e1 = D.E1 + (d != 1), e2 = D.E2 + (d != 2);
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
   if (jk >= e1 * e2) return;
@@ -360,8 +370,13 @@ __device__ inline bool flux_density(const Dims &D, const DevState &S, const DevG
 // Wind-front diffusive EMF on the outer shell's j and k edges,
 // cubedsphere_earth_boundary.c:298-379.
 __global__ void k_earth_emf_diffusive(Dims D, DevState S, DevGeom G, EarthDev E,
-                                      double tmid, double dt, DevStatus *st) {
+                                      double tmid, double dt, const StepParams *prm,
+                                      DevStatus *st) {
   if (failed(st)) return;
+  if (prm) {
+    tmid = prm->time + 0.5 * prm->dt;
+    dt = prm->dt;
+  }
   const int w1 = D.n + 1;
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
   if (jk >= w1 * w1) return;
@@ -436,19 +451,20 @@ inline unsigned blocks(long long n) { return (unsigned)((n + 127) / 128); }
 
 }  // namespace
 
-void launch_earth_radial(const Ctx &X, const EarthDev &E, double current_time,
-                         double previous_time, cudaStream_t s) {
+void launch_earth_radial(const Ctx &X, const EarthStep &es, cudaStream_t s) {
   const Dims &D = X.D;
+  const EarthDev &E = *es.dev;
+  const StepParams *prm = es.device_times ? X.params : nullptr;
   const dim3 gc(blocks((long long)D.E1 * D.E2), 2 * D.g, kFaces);
-  k_earth_cells<<<gc, 128, 0, s>>>(D, X.S, E, current_time, 0, X.status);
-  k_earth_cells<<<gc, 128, 0, s>>>(D, X.S, E, previous_time, 1, X.status);
+  k_earth_cells<<<gc, 128, 0, s>>>(D, X.S, E, es.current_time, 0, prm, X.status);
+  k_earth_cells<<<gc, 128, 0, s>>>(D, X.S, E, es.previous_time, 1, prm, X.status);
   const Tile t{128, 1};
   for (int old = 0; old < 2; ++old) {
-    const double time = old ? previous_time : current_time;
+    const double time = old ? es.previous_time : es.current_time;
     for (int d = 0; d < 3; ++d) {
       const long long pl = (long long)(D.E1 + (d == 1)) * (D.E2 + (d == 2));
-      k_earth_faces<<<dim3(blocks(pl), 2 * D.g, kFaces), 128, 0, s>>>(D, X.S, X.G, E, d,
-                                                                       time, old, X.status);
+      k_earth_faces<<<dim3(blocks(pl), 2 * D.g, kFaces), 128, 0, s>>>(
+          D, X.S, X.G, E, d, time, old, prm, X.status);
     }
     k_earth_recover<<<tile_grid(D.E0, D.E1, D.E2, t), tile_block(t), 0, s>>>(D, X.S, X.G,
                                                                               old, X.status);
@@ -461,17 +477,18 @@ void launch_earth_trap(const Ctx &X, cudaStream_t s) {
   k_earth_trap<<<dim3(blocks((long long)X.D.n * X.D.n), 1, kFaces), 128, 0, s>>>(X.D, X.S);
 }
 
-void launch_earth_emf(const Ctx &X, const EarthDev &E, double step_time, double step_dt,
-                      cudaStream_t s) {
+void launch_earth_emf(const Ctx &X, const EarthStep &es, cudaStream_t s) {
   const Dims &D = X.D;
-  const double tmid = step_time + 0.5 * step_dt;
+  const EarthDev &E = *es.dev;
+  const StepParams *prm = es.device_times ? X.params : nullptr;
+  const double tmid = es.step_time + 0.5 * es.step_dt;
   for (int d = 0; d < 3; ++d) {
     const long long pl = (long long)(D.E1 + (d != 1)) * (D.E2 + (d != 2));
-    k_earth_emf_outer<<<dim3(blocks(pl), 4, kFaces), 128, 0, s>>>(D, X.S, E, d, tmid,
+    k_earth_emf_outer<<<dim3(blocks(pl), 4, kFaces), 128, 0, s>>>(D, X.S, E, d, tmid, prm,
                                                                    X.status);
   }
   k_earth_emf_diffusive<<<dim3(blocks((long long)(D.n + 1) * (D.n + 1)), 1, kFaces), 128, 0,
-                          s>>>(D, X.S, X.G, E, tmid, step_dt, X.status);
+                          s>>>(D, X.S, X.G, E, tmid, es.step_dt, prm, X.status);
   for (int d = 1; d < 3; ++d) {
     const long long pl = (long long)(D.E1 + (d != 1)) * (D.E2 + (d != 2));
     k_earth_emf_inner<<<dim3(blocks(pl), 1, kFaces), 128, 0, s>>>(D, X.S, E, d, X.status);
@@ -875,7 +892,8 @@ int fill_radial(const gamera_no_grid grid[GAMERA_CS_FACE_COUNT],
   gcs_earth *e = gcs::earth_for(*C, grid, b, true);
   if (!e || C->upload_state(storage) != 0) return -1;
   C->reset_status_async();
-  gcs::launch_earth_radial(C->X, e->dev, t, tprev, C->stream);
+  const gcs::EarthStep es{&e->dev, t, tprev, t, 0.0, 0};
+  gcs::launch_earth_radial(C->X, es, C->stream);
   gcs::DevStatus s;
   if (cudaGetLastError() != cudaSuccess || C->read_status(&s) != 0 || s.first != 0) {
     C->reset_status_async();

@@ -48,16 +48,19 @@ struct EarthDev {
 
 // Times of one step with the device Earth boundary: the radial fill at
 // (current, previous) time, the EMF at step_time + step_dt / 2.
+// With device_times the times are read from the context's step parameters
+// instead (driver mode): current = time, previous = time - dt_prev (time on
+// the first step), step time = time, step dt = dt, as the reference driver
+// sets them (test_cubedsphere_dipole_background.c:655-692).
 struct EarthStep {
   const EarthDev *dev;
   double current_time, previous_time, step_time, step_dt;
+  int device_times;
 };
 
-void launch_earth_radial(const Ctx &X, const EarthDev &E, double current_time,
-                         double previous_time, cudaStream_t s);
+void launch_earth_radial(const Ctx &X, const EarthStep &es, cudaStream_t s);
 void launch_earth_trap(const Ctx &X, cudaStream_t s);
-void launch_earth_emf(const Ctx &X, const EarthDev &E, double step_time, double step_dt,
-                      cudaStream_t s);
+void launch_earth_emf(const Ctx &X, const EarthStep &es, cudaStream_t s);
 
 struct Context;
 // The device boundary the drop-in step and the host entry points use for

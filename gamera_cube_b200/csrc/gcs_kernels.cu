@@ -334,7 +334,10 @@ __global__ void k_next_dt(StepParams *prm, DevStatus *st, double fraction) {
   st->cfl_min_bits = (unsigned long long)__double_as_longlong(DBL_MAX);
 }
 
-__global__ void k_count_step(StepParams *prm) { prm->step += 1; }
+__global__ void k_count_step(StepParams *prm) {
+  prm->time += prm->dt;
+  prm->step += 1;
+}
 
 // ---------------------------------------------------------------------------
 // Host-side launchers.

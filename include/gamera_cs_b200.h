@@ -447,6 +447,17 @@ int gcs_context_step_earth(gcs_context *ctx, gcs_earth *earth,
                            const gamera_no_advance_options *options,
                            double predictor_ratio, double dt, double current_time,
                            double previous_time);
+/* The driver loop of gcs_context_run with the device Earth boundary: its
+ * times come from the device step parameters (current time t, previous
+ * t - dt_prev or t on the first step, EMF at t + dt/2), so with use_graph
+ * each step is one CUDA graph launch and needs no host synchronisation.
+ * The simulation time starts at 0 with the context's first driver step.
+ * The MI potential (boundary->mi at creation) is the one current at the
+ * call. */
+int gcs_context_run_earth(gcs_context *ctx, gcs_earth *earth,
+                          const gamera_no_advance_options *options,
+                          const gamera_no_timestep_options *timestep, double dt_fraction,
+                          int steps, int use_graph);
 
 /* Analysis output (cubedsphere/cubedsphere_analysis_hdf5.c:299-355,
  * cubedsphere/docs/OUTPUT_DATA_MODEL.md).  The frame of a face is float32

@@ -401,3 +401,45 @@ def test_drop_in_step_with_mi_coupled_wall(lib, strict):
         lib.gamera_cs_mi_dipole_destroy(views[1])
         ref.close()
         gpu.close()
+
+
+def test_earth_driver_loop_matches_stepwise(lib):
+    """gcs_context_run_earth (device times, one CUDA graph per step) equals
+    the same steps driven from the host with the reference driver's dt rule
+    and times, bit for bit."""
+    keep = []
+    startup = abi.EarthStartup()
+    startup.gamma = 5.0 / 3.0
+    wind = wind_series(keep)
+    o, t = abi.AdvanceOptions(), abi.TimestepOptions()
+    assert lib.gcs_case_options(2, C.byref(o), C.byref(t)) == 0
+    a = lib.gcs_context_create_case(2, 20, 10, 5)
+    b = lib.gcs_context_create_case(2, 20, 10, 5)
+    ea, eb = C.c_void_p(), C.c_void_p()
+    try:
+        for ctx, e in ((a, ea), (b, eb)):
+            bd = boundary(startup, wind, None, 0)
+            keep.append(bd)
+            assert lib.gcs_earth_create_case(ctx, C.byref(bd), C.byref(e)) == 0
+        assert lib.gcs_context_run_earth(a, ea, C.byref(o), C.byref(t), 0.5, 2, 1) == 0
+        assert lib.gcs_context_run_earth(a, ea, C.byref(o), C.byref(t), 0.5, 2, 1) == 0
+        assert lib.gcs_context_sync(a) == 0
+        time, dt_prev = 0.0, 0.0
+        for s in range(4):
+            local = C.c_double()
+            assert lib.gcs_context_timestep(b, C.byref(t), C.byref(local)) == 0
+            dt = 0.5 * local.value if s == 0 else min(0.5 * local.value, 1.25 * dt_prev)
+            ratio = 0.0 if s == 0 else 0.5 * dt / dt_prev
+            prev = time if s == 0 else time - dt_prev
+            assert lib.gcs_context_step_earth(b, eb, C.byref(o), ratio, dt, time, prev) == 0
+            time += dt
+            dt_prev = dt
+        from tests.test_ensemble_gpu import download, assert_same_state
+        ha, hb = download(lib, a), download(lib, b)
+        assert_same_state(ha, hb)
+    finally:
+        for e in (ea, eb):
+            if e:
+                lib.gcs_earth_destroy(e)
+        lib.gcs_context_destroy(a)
+        lib.gcs_context_destroy(b)

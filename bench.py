@@ -463,7 +463,7 @@ def run_earth(lib, torch, device, args, dist, ctx):
                         "constant upstream monitor" % (act[1], act[2], act[0]),
             "call": "gcs_context_run_earth (device driver loop, one CUDA graph per step)",
             "boundary_device_bytes": nbytes,
-            "gpu_launches_per_step": 24 + 19}
+            "gpu_launches_per_step": 24 + 18}
 
 
 ENS_SEED = 2024

@@ -273,28 +273,32 @@ __global__ void k_earth_faces(Dims D, DevState S, DevGeom G, EarthDev E, int d,
   P[c] = wt * wf + (1.0 - wt) * P[f * D.Nn + D.node(si, j, k)];
 }
 
-// Cell B (old = 0) or old cell B (old = 1) of every cell from the face
+// Cell B and old cell B of every cell from the face fluxes and old face
 // fluxes (nonorthogonal_step.c:310-358 as called at
-// cubedsphere_earth_boundary.c:169-172).
-__global__ void k_earth_recover(Dims D, DevState S, DevGeom G, int old, DevStatus *st) {
+// cubedsphere_earth_boundary.c:169-172 after each field's face fill; the
+// two fills touch disjoint arrays, so one pass recovers both and reads the
+// recovery map once).
+__global__ void k_earth_recover(Dims D, DevState S, DevGeom G, DevStatus *st) {
   if (failed(st)) return;
   int f, i, j, k;
   const Box b{0, 0, 0, D.E1, D.E2, D.E0};
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const long long c = f * D.Nn + D.node(i, j, k);
-  double *const *P = old ? S.Po : S.P;
-  double phi[6], bn[3];
   const long long sdir[3] = {D.stride(0), D.stride(1), 1};
-  for (int d = 0; d < 3; ++d) {
-    phi[2 * d] = P[d][c];
-    phi[2 * d + 1] = P[d][c + sdir[d]];
+  for (int old = 0; old < 2; ++old) {
+    double *const *P = old ? S.Po : S.P;
+    double phi[6], bn[3];
+    for (int d = 0; d < 3; ++d) {
+      phi[2 * d] = P[d][c];
+      phi[2 * d + 1] = P[d][c + sdir[d]];
+    }
+    if (!recover_cell(G, c, phi, bn)) {
+      fail(st, kStageHost, 0, f, i, j, k);
+      return;
+    }
+    double *const *B = old ? S.Bo : S.B;
+    for (int m = 0; m < 3; ++m) B[m][c] = bn[m];
   }
-  if (!recover_cell(G, c, phi, bn)) {
-    fail(st, kStageHost, 0, f, i, j, k);
-    return;
-  }
-  double *const *B = old ? S.Bo : S.B;
-  for (int m = 0; m < 3; ++m) B[m][c] = bn[m];
 }
 
 // dB/dr = 0 in the inner ghost cells (cubedsphere_earth_boundary.c:173-182).
@@ -466,11 +470,12 @@ void launch_earth_radial(const Ctx &X, const EarthStep &es, cudaStream_t s) {
       k_earth_faces<<<dim3(blocks(pl), 2 * D.g, kFaces), 128, 0, s>>>(
           D, X.S, X.G, E, d, time, old, prm, X.status);
     }
-    k_earth_recover<<<tile_grid(D.E0, D.E1, D.E2, t), tile_block(t), 0, s>>>(D, X.S, X.G,
-                                                                              old, X.status);
+  }
+  k_earth_recover<<<tile_grid(D.E0, D.E1, D.E2, t), tile_block(t), 0, s>>>(D, X.S, X.G,
+                                                                            X.status);
+  for (int old = 0; old < 2; ++old)
     k_earth_copy_inner<<<dim3(blocks((long long)D.E1 * D.E2), D.g, kFaces), 128, 0, s>>>(
         D, X.S, old);
-  }
 }
 
 void launch_earth_trap(const Ctx &X, cudaStream_t s) {

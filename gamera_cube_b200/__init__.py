@@ -98,6 +98,7 @@ def _load(path=None):
         "gcs_mi_tensor_plan_buffers": (C.c_int, [C.c_void_p] + [P(C.c_void_p)] * 4),
         "gcs_mi_tensor_plan_upload": (C.c_int, [C.c_void_p] + [P(C.c_double)] * 4),
         "gcs_mi_tensor_solve_async": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "gcs_mi_tensor_plan_set_ordering": (C.c_int, [C.c_void_p, C.c_int]),
         "gcs_mi_tensor_results": (C.c_int, [C.c_void_p, P(abi.MiSolverStats),
                                             P(C.c_int)]),
         "gcs_mi_plan_create": (C.c_int, [P(abi.MiSolverConfig), C.c_int,

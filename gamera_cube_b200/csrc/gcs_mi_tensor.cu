@@ -93,6 +93,7 @@ struct TSys {
   int *fault;   // set when a sweep copy never arrived
   gamera_mi_solver_stats *stats;
   int *status;  // 0 converged, 1 not converged, 2 non-finite FAC, 3 sweep copy lost
+  int colored;  // 1: multicolour SSOR by the whole cluster instead of the wavefront
 };
 
 // Position of row r inside a diagonal of Rp = 32 M rows: the sweep warp's
@@ -398,6 +399,14 @@ __device__ __forceinline__ double apply_at(const TSys &S, const double *p, size_
   return S.dg[k] * p[k] + S.lo[k] * lv + S.up[k] * uv + S.ll[k] * p[kw] + S.lu[k] * p[ke];
 }
 
+// Colour of grid point (row, j) in the multicolour SSOR: the pole first,
+// then (row + j) parity off the seam column and row parity on it (the last
+// longitude, whose periodic neighbour j = 0 has the same (row + j) parity
+// when np is odd); no two points of one colour are stencil neighbours.
+__device__ __forceinline__ int tcolor(int row, int j, int np) {
+  return j + 1 < np ? ((row + j) & 1) : 2 + (row & 1);
+}
+
 // Partial dot products of one thread.
 template <int N>
 struct Acc {
@@ -650,6 +659,91 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor(TSys S) {
       *S.pole_sum = psum;
     }
   };
+  // The reference's triangular SSOR (nonorthogonal_mi.c:910-964) with the
+  // unknowns ordered by colour (tcolor) instead of row by row: within a
+  // colour every update is independent, so the whole cluster sweeps one
+  // colour at a time.  A different ordering of the same splitting: the
+  // preconditioner, and so the iteration count, differ from the reference's.
+  auto colored_ssor = [&](const double *in, double *out) {
+    double *fw = S.fw;
+    if (lead) fw[0] = in[0];
+    cl.sync();
+    const unsigned half = (unsigned)(np / 2);  // colour-0/1 slots per row
+    for (int dir = 0; dir < 2; ++dir) {
+      const double *src = dir == 0 ? fw : out;
+      double *dst = dir == 0 ? fw : out;
+      for (int ci = 0; ci < 4; ++ci) {
+        const int c = dir == 0 ? ci : 3 - ci;
+        // the colour's points, enumerated directly: (row, 2 m + parity) off
+        // the seam column for colours 0 and 1, rows of one parity on it for
+        // colours 2 and 3
+        const unsigned n = c < 2 ? (unsigned)R * half : (unsigned)(R - (c - 2) + 1) / 2;
+        for (unsigned t0 = g; t0 < n; t0 += kB * G) {
+          size_t kk[kB];
+          bool on[kB];
+          double v[kB], rd[kB], cf[kB][4], nb[kB][4];
+#pragma unroll
+          for (int b = 0; b < kB; ++b) {
+            const unsigned tt = t0 + b * G;
+            int row = 0, j = 0;
+            if (c < 2) {
+              row = (int)(tt / half);
+              j = 2 * (int)(tt - (unsigned)row * half) + ((c + row) & 1);
+              on[b] = tt < n && j < np - 1;
+            } else {
+              row = 2 * (int)tt + (c - 2);
+              j = np - 1;
+              on[b] = tt < n && row < R;
+            }
+            kk[b] = 0;
+            v[b] = rd[b] = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) cf[b][q] = nb[b][q] = 0.0;
+            if (!on[b]) continue;
+            const size_t k = sidx(Rp, row, j);
+            const size_t q = (size_t)row_pos(Rp, row);
+            const int jm = j == 0 ? np - 1 : j - 1, jp = j + 1 == np ? 0 : j + 1;
+            kk[b] = k;
+            v[b] = dir == 0 ? in[k] : fw[k];
+            rd[b] = S.rdg[k];
+            // neighbours of an earlier colour (forward) or a later one (reverse)
+            const int cn[4] = {row == 0 ? -1 : tcolor(row - 1, j, np),
+                               row + 1 < R ? tcolor(row + 1, j, np) : c,
+                               tcolor(row, jm, np), tcolor(row, jp, np)};
+            const size_t kn[4] = {row == 0 ? 0 : k - q - Rp + row_pos(Rp, row - 1),
+                                  row + 1 < R ? k - q + Rp + row_pos(Rp, row + 1) : k,
+                                  j == 0 ? k + (size_t)(np - 1) * Rp : k - Rp,
+                                  j + 1 == np ? k - (size_t)(np - 1) * Rp : k + Rp};
+            const double *co[4] = {S.lo, S.up, S.ll, S.lu};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              if (dir == 0 ? cn[e] < c : cn[e] > c) {
+                cf[b][e] = co[e][k];
+                nb[b][e] = src[kn[e]];
+              }
+            }
+          }
+#pragma unroll
+          for (int b = 0; b < kB; ++b) {
+            if (!on[b]) continue;
+            double x = v[b];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) x -= cf[b][e] * rd[b] * nb[b][e];
+            dst[kk[b]] = x;
+          }
+        }
+        cl.sync();
+      }
+    }
+    // pole (nonorthogonal_mi.c:958-963): (dg0 fw0 + sum pe_j out(1, j)) / dg0
+    double ps[1] = {0.0};
+    for (unsigned jj = g; jj < (unsigned)np; jj += G) ps[0] += S.pe[jj] * out[sidx(Rp, 0, jj)];
+    red.template sum<1>(cl, ps);
+    if (lead) {
+      out[0] = (dg0 * fw[0] + ps[0]) / dg0;
+      *S.pole_sum = ps[0];
+    }
+  };
   // BiCGStab (nonorthogonal_mi.c:1040-1128)
   for (int it = 1; !conv && it <= max_iter; ++it) {
     if (!isfinite(rho) || fabs(rho) <= DBL_MIN || !isfinite(omega) || fabs(omega) <= DBL_MIN)
@@ -681,7 +775,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor(TSys S) {
       S.pin[0] = s * rdg0;
     }
     cl.sync();
-    if (sweeper) ssor(S.pin, S.psv);
+    if (S.colored)
+      colored_ssor(S.pin, S.psv);
+    else if (sweeper)
+      ssor(S.pin, S.psv);
     cl.sync();
     if (*(volatile int *)S.fault) break;
     Acc<1> d2;
@@ -743,7 +840,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor(TSys S) {
       conv = 1;
       break;
     }
-    if (sweeper) ssor(S.pin, S.pm);
+    if (S.colored)
+      colored_ssor(S.pin, S.pm);
+    else if (sweeper)
+      ssor(S.pin, S.pm);
     cl.sync();
     if (*(volatile int *)S.fault) break;
     Acc<2> d4;
@@ -1079,6 +1179,12 @@ int gcs_mi_tensor_plan_create(const gamera_mi_solver_config *config,
   if (!plan) return -1;
   *plan = plan_create(config);
   return *plan ? 0 : -1;
+}
+
+int gcs_mi_tensor_plan_set_ordering(gcs_mi_tensor_plan *plan, int colored) {
+  if (!plan || (colored != 0 && colored != 1)) return -1;
+  plan->sys.colored = colored;
+  return 0;
 }
 
 void gcs_mi_tensor_plan_destroy(gcs_mi_tensor_plan *plan) {

@@ -606,6 +606,13 @@ int gcs_mi_tensor_plan_upload(gcs_mi_tensor_plan *plan, const double *fac,
                               const double *pedersen, const double *hall,
                               const double *potential);
 int gcs_mi_tensor_solve_async(gcs_mi_tensor_plan *plan, void *stream);
+/* Ordering of the SSOR preconditioner (no reference counterpart): 0 the
+ * reference's row-by-row sweeps (default; one warp advances a wavefront),
+ * 1 the same splitting with the unknowns ordered by colour (pole; (row +
+ * longitude) parity off the seam column; row parity on it), each colour
+ * swept by the whole cluster at once.  Both solve to the configured
+ * tolerance; the iteration counts differ. */
+int gcs_mi_tensor_plan_set_ordering(gcs_mi_tensor_plan *plan, int colored);
 int gcs_mi_tensor_results(gcs_mi_tensor_plan *plan, gamera_mi_solver_stats *stats,
                           int *status);
 /* Ionosphere coupling of a device-built case (gcs_context_create_case with

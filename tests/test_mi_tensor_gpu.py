@@ -148,3 +148,72 @@ def test_tensor_rejects_bad_input():
     assert L.gamera_mi_solve_conductance_tensor(
         C.byref(bad), ptr(d["fac"]), ptr(d["pedersen"]), ptr(d["hall"]), ptr(pot),
         C.byref(st)) == -1
+
+
+def plan_solve(case, colored):
+    """The device tensor plan with the given SSOR ordering; returns the
+    potential, stats, status and device milliseconds of one solve."""
+    import torch
+    from gamera_cube_b200 import abi
+    L = glib()
+    cudart = C.CDLL("libcudart.so.12")
+    plan = C.c_void_p()
+    assert L.gcs_mi_tensor_plan_create(C.byref(case.config), C.byref(plan)) == 0
+    try:
+        assert L.gcs_mi_tensor_plan_set_ordering(plan, colored) == 0
+        pot = case.potential.copy()
+        assert L.gcs_mi_tensor_plan_upload(plan, ptr(case.fac), ptr(case.pedersen),
+                                           ptr(case.hall), ptr(pot)) == 0
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s = torch.cuda.current_stream()
+        a.record(s)
+        assert L.gcs_mi_tensor_solve_async(plan, C.c_void_p(s.cuda_stream)) == 0
+        b.record(s)
+        st, status = abi.MiSolverStats(), C.c_int()
+        assert L.gcs_mi_tensor_results(plan, C.byref(st), C.byref(status)) == 0
+        b.synchronize()
+        bufs = [C.c_void_p() for _ in range(4)]
+        assert L.gcs_mi_tensor_plan_buffers(plan, *[C.byref(x) for x in bufs]) == 0
+        host = np.zeros(case.potential.shape)
+        assert cudart.cudaMemcpy(C.c_void_p(host.ctypes.data),
+                                 bufs[3], C.c_size_t(host.nbytes),
+                                 2) == 0
+        return host, st, status.value, a.elapsed_time(b)
+    finally:
+        L.gcs_mi_tensor_plan_destroy(plan)
+
+
+@pytest.mark.parametrize("npl,nt,hemisphere", [
+    (361, 181, 1),   # production grid, odd longitude count (seam colours)
+    (40, 250, -1),
+    (12, 70, 1),
+    (8, 12, 1),
+])
+def test_colored_ordering_converges_to_the_reference_solution(npl, nt, hemisphere):
+    """The multicolour SSOR ordering: converged, and as close to the
+    oracle's 1e-12 solve as the reference's own 1e-8 solve is (see
+    test_tensor_grid_shapes); iteration count and time recorded."""
+    from gamera_cube_b200 import cases
+    case = cases.mi_case(npl, nt, seed=npl + nt, hemisphere=hemisphere,
+                         max_iterations=20000)
+    tight = cases.mi_case(npl, nt, seed=npl + nt, hemisphere=hemisphere,
+                          max_iterations=200000, rel_tol=1e-12)
+    d = {"fac": case.fac, "pedersen": case.pedersen, "hall": case.hall}
+    O = oracle_cases.lib()
+    rc, truth, _ = solve(O, O.gcso_mi_solve_conductance_tensor, tight.config, d,
+                         case.potential)
+    assert rc == 0
+    rc, ref, ref_st = solve(O, O.gcso_mi_solve_conductance_tensor, case.config, d,
+                            case.potential)
+    assert rc == 0
+    pot, st, status, ms = plan_solve(case, 1)
+    assert status == 0 and st.converged == 1, (status, st.iterations)
+    scale = np.abs(truth).max()
+    ref_err = np.abs(ref - truth).max()
+    assert np.abs(pot - truth).max() <= 2.0 * ref_err + 5e-8 * scale
+    # as converged as the reference's own 1e-8 solve, in one residual norm
+    res, _ = tensor_residual(case.config, case.fac, case.pedersen, case.hall, pot)
+    ref_res, _ = tensor_residual(case.config, case.fac, case.pedersen, case.hall, ref)
+    assert res <= 2.0 * ref_res, (res, ref_res)
+    print("colored %dx%d: %d iterations (reference ordering %d), %.2f ms"
+          % (nt, npl, st.iterations, ref_st.iterations, ms))

@@ -450,6 +450,25 @@ def run_earth(lib, torch, device, args, dist, ctx):
     stop.synchronize()
     ok = ok and lib.gcs_context_sync(ctx) == 0
     ms = max_over_ranks(start.elapsed_time(stop), dist, device)
+    # the same loop with the Earth drivers' post-step pressure control
+    # (gamma, 1e-6, 1e-8, c = 10, 1e-3, 1e-7: the production arguments)
+    pc = abi.PressureControl(5.0 / 3.0, 1e-6, 1e-8, 10.0, 1e-3, 1e-7)
+    ok = ok and lib.gcs_context_set_pressure_control(ctx, None, C.byref(pc)) == 0
+    ok = ok and lib.gcs_context_run_earth(ctx, earth, C.byref(opts), C.byref(ts), 0.5, 3, 1) == 0
+    ok = ok and lib.gcs_context_sync(ctx) == 0
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    start.record(stream)
+    ok = ok and lib.gcs_context_run_earth(ctx, earth, C.byref(opts), C.byref(ts), 0.5,
+                                          args.earth_steps, 1) == 0
+    stop.record(stream)
+    stop.synchronize()
+    ok = ok and lib.gcs_context_sync(ctx) == 0
+    ms_pc = max_over_ranks(start.elapsed_time(stop), dist, device)
+    pc_low, pc_hot = C.c_size_t(), C.c_size_t()
+    ok = ok and lib.gcs_context_pressure_control_stats(ctx, C.byref(pc_low), C.byref(pc_hot),
+                                                       None, None, 1) == 0
+    ok = ok and lib.gcs_context_set_pressure_control(ctx, None, None) == 0
     act = (C.c_size_t * 3)()
     g = C.c_size_t()
     lib.gcs_context_dims(ctx, act, C.byref(g))
@@ -463,7 +482,13 @@ def run_earth(lib, torch, device, args, dist, ctx):
                         "constant upstream monitor" % (act[1], act[2], act[0]),
             "call": "gcs_context_run_earth (device driver loop, one CUDA graph per step)",
             "boundary_device_bytes": nbytes,
-            "gpu_launches_per_step": 24 + 18}
+            "gpu_launches_per_step": 24 + 18,
+            "with_pressure_control": {
+                "ms_per_step": ms_pc / args.earth_steps,
+                "arguments": "gamma 5/3, floors 1e-6/1e-8, c 10, low density 1e-3, "
+                             "low-density sound speed 1e-7",
+                "low_density_cells": pc_low.value, "high_sound_speed_cells": pc_hot.value,
+                "gpu_launches_per_step": 24 + 18 + 2}}
 
 
 ENS_SEED = 2024

@@ -248,6 +248,15 @@ class WindDriver(C.Structure):
                 ("temperature_k", C.c_double), ("bz_nt", C.c_double)]
 
 
+class PressureControl(C.Structure):
+    """gcs_pressure_control: the arguments of gamera_no_apply_pressure_control
+    after dt (nonorthogonal_step.h:26-32)."""
+    _fields_ = [("gamma", C.c_double), ("density_floor", C.c_double),
+                ("pressure_floor", C.c_double), ("light_speed", C.c_double),
+                ("low_density_threshold", C.c_double),
+                ("low_density_sound_speed", C.c_double)]
+
+
 class EnsembleConfig(C.Structure):
     """gcs_ensemble_config."""
     _fields_ = [("count", C.c_int), ("nr", C.POINTER(C.c_size_t)),
@@ -303,6 +312,15 @@ def ensemble_signatures():
         "gcs_context_write_analysis": (C.c_int, [C.c_void_p, C.c_char_p, C.c_long, C.c_long,
                                                  C.c_double, C.c_double, C.c_double,
                                                  P(Grid)]),
+        "gcs_context_pressure_control": (C.c_int, [C.c_void_p, P(Grid), C.c_double,
+                                                   P(PressureControl), P(C.c_size_t),
+                                                   P(C.c_size_t), P(C.c_double),
+                                                   P(C.c_double)]),
+        "gcs_context_set_pressure_control": (C.c_int, [C.c_void_p, P(Grid),
+                                                       P(PressureControl)]),
+        "gcs_context_pressure_control_stats": (C.c_int, [C.c_void_p, P(C.c_size_t),
+                                                         P(C.c_size_t), P(C.c_double),
+                                                         P(C.c_double), C.c_int]),
     })
     return sig
 

@@ -42,7 +42,7 @@ const char *kStageNames[] = {
     "kinetic_fluid",  "kinetic_maxwell", "emergency",       "edge_geometry",
     "edge_velocity",  "transverse_field", "edge_density",   "compute_edge_emf",
     "boris_after_hydro", "recover_update", "recover_B",     "timestep",
-    "host_callback",  "solve_edge_field", "options"};
+    "host_callback",  "solve_edge_field", "options",        "pressure_control"};
 
 // Option checks of the reference step and of each stage it calls
 // (cubedsphere_step.c:23-47, nonorthogonal_sweep.c:48-62, 209-221,
@@ -228,6 +228,7 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   }
   const gcs::Ctx &X = C.X;
   cudaStream_t s = C.stream;
+  const bool post_control = driver_mode && C.pc_on;
   Marker mk{ctx};
   mk.begin();
   gcs::launch_seam_sync(X, 1, s);
@@ -284,8 +285,14 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   if (O.u_mhd) {
     gcs::launch_seam_sync(X, 1, s);
     mk.mark(kSlotSeamPhiFinal);
-    gcs::launch_recover(X, O, driver_mode, s);
+    gcs::launch_recover(X, O, driver_mode && !post_control, s);
     mk.mark(kSlotRecover);
+  }
+  if (post_control) {
+    // the Earth drivers' post-step pressure control with this step's dt,
+    // then the CFL step of the controlled state
+    gcs::launch_pressure_control(C, C.pc, 0.0, true, s);
+    gcs::launch_timestep(X, O, s);
   }
   if (driver_mode) {
     gcs::launch_count_step(X, s);
@@ -1064,6 +1071,11 @@ int context_run(gcs_context *ctx, const gamera_no_advance_options *options,
     for (int f = 0; f < gcs::kTileFamilies; ++f)
       key = (key ^ (unsigned long long)(C.X.tile[f].bx * 64 + C.X.tile[f].by)) *
             1099511628211ULL;
+    if (C.pc_on) {
+      const unsigned char *pb = (const unsigned char *)&C.pc;
+      for (size_t q = 0; q < sizeof(C.pc); ++q) key = (key ^ pb[q]) * 1099511628211ULL;
+      key = (key ^ 0x50524553ULL) * 1099511628211ULL;
+    }
     if (!C.graph_exec || C.graph_key != key) {
       if (C.graph_exec) cudaGraphExecDestroy(C.graph_exec);
       C.graph_exec = nullptr;

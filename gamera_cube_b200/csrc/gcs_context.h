@@ -24,6 +24,12 @@ WindInit case_wind(int kind);
 WindInit driven_wind(double density_cm3, double velocity_x_kms, double temperature_k,
                      double bz_nt);
 
+// Arguments of the post-step pressure control (nonorthogonal_step.h:26-32).
+struct PressureControl {
+  double gamma, density_floor, pressure_floor, light_speed, low_density_threshold,
+      low_density_sound_speed;
+};
+
 struct Context {
   Ctx X;
   cudaStream_t stream = nullptr;
@@ -53,6 +59,12 @@ struct Context {
   int win_layers = 0;
   std::vector<gamera_no_vec3> win_centroid[kFaces];
   std::vector<gamera_no_vec3> win_vertex[kFaces];
+  // Post-step pressure control of the driver loop (gcs_pressure.cu): the
+  // dipole line length of every active cell and the device counters.
+  PressureControl pc{};
+  int pc_on = 0;
+  double *pc_dipole = nullptr;
+  void *pc_stats = nullptr;
   // per-stage timing (profiling mode)
   int profiling = 0;
   double stage_ms[16] = {0};
@@ -108,6 +120,12 @@ struct Context {
     return true;
   }
 };
+
+// gcs_pressure.cu
+int pressure_prepare(Context &C, const gamera_no_grid *grid);
+int pressure_reset_async(Context &C);
+void launch_pressure_control(Context &C, const PressureControl &pc, double dt,
+                             bool from_params, cudaStream_t s);
 
 }  // namespace gcs
 

@@ -158,6 +158,7 @@ enum Stage : int {
   kStageHost = 16,
   kStageSolveEdge = 17,
   kStageOptions = 18,
+  kStagePressureControl = 19,
 };
 
 struct DevStatus {

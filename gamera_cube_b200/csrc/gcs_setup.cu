@@ -334,6 +334,10 @@ void Context::release() {
   if (staging_host) cudaFreeHost(staging_host);
   if (X.params) cudaFree(X.params);
   if (X.status) cudaFree(X.status);
+  if (pc_dipole) cudaFree(pc_dipole);   // one allocation with pc_stats
+  pc_dipole = nullptr;
+  pc_stats = nullptr;
+  pc_on = 0;
   if (stream) cudaStreamDestroy(stream);
   pool = nullptr;
   plans = nullptr;

@@ -237,7 +237,8 @@ enum {
   GCS_STAGE_TIMESTEP = 15,
   GCS_STAGE_HOST = 16,
   GCS_STAGE_SOLVE_EDGE = 17,
-  GCS_STAGE_OPTIONS = 18
+  GCS_STAGE_OPTIONS = 18,
+  GCS_STAGE_PRESSURE_CONTROL = 19
 };
 
 /* Build a device context from a host grid in the reference layout
@@ -458,6 +459,46 @@ int gcs_context_run_earth(gcs_context *ctx, gcs_earth *earth,
                           const gamera_no_advance_options *options,
                           const gamera_no_timestep_options *timestep, double dt_fraction,
                           int steps, int use_graph);
+
+/* Post-step pressure control of the Earth drivers
+ * (nonorthogonal/src/nonorthogonal/nonorthogonal_step.h:26-32
+ * gamera_no_apply_pressure_control, called after each step by
+ * cubedsphere/tests/test_cubedsphere_mpi_earth_tile.c:459-481 with gamma,
+ * 1e-6, 1e-8, 10, 1e-3, 1e-7).  The arguments after dt, same meaning. */
+typedef struct gcs_pressure_control {
+  double gamma;
+  double density_floor;
+  double pressure_floor;
+  double light_speed;
+  double low_density_threshold;
+  double low_density_sound_speed;
+} gcs_pressure_control;
+/* gamera_no_apply_pressure_control over the active cells of all six faces
+ * of a device-resident state, on the device: counts summed over the faces,
+ * maxima over them.  The dipole line lengths come from `grid` (the host
+ * grid of the context) or, for a device-built case, grid NULL, from its
+ * device-built centroids; computed on the first call and kept.  -1 on an
+ * invalid argument or a failed cell, as the reference (other cells
+ * updated). */
+int gcs_context_pressure_control(gcs_context *ctx, const gamera_no_grid *grid, double dt,
+                                 const gcs_pressure_control *config,
+                                 size_t *low_density_cell_count,
+                                 size_t *high_sound_speed_cell_count,
+                                 double *maximum_sound_speed, double *maximum_pressure);
+/* Run the pressure control after every step of the device driver loop
+ * (gcs_context_run, gcs_context_run_earth; inside the step's CUDA graph,
+ * dt from the step parameters, the next CFL step from the controlled
+ * state); config NULL turns it off.  Counts accumulate over the steps and
+ * maxima are taken over them until read with reset; a failed cell fails
+ * the step (stage "pressure_control"). */
+int gcs_context_set_pressure_control(gcs_context *ctx, const gamera_no_grid *grid,
+                                     const gcs_pressure_control *config);
+/* Counters of the driver-loop pressure control; 0, 1 when a cell failed,
+ * -1 on error.  reset != 0 zeroes them (stream-ordered). */
+int gcs_context_pressure_control_stats(gcs_context *ctx, size_t *low_density_cell_count,
+                                       size_t *high_sound_speed_cell_count,
+                                       double *maximum_sound_speed, double *maximum_pressure,
+                                       int reset);
 
 /* Analysis output (cubedsphere/cubedsphere_analysis_hdf5.c:299-355,
  * cubedsphere/docs/OUTPUT_DATA_MODEL.md).  The frame of a face is float32

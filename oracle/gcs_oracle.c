@@ -765,6 +765,64 @@ static int s_p2c(const prim *p, double g, double rf, double pf, double u[5]) {
   return 0;
 }
 
+/* nonorthogonal_step.c:74-171: post-step pressure control over the cells
+ * [lower, upper) of one face (serial; the counts and maxima are
+ * order-independent). */
+int gcso_apply_pressure_control(gamera_no_storage *s, const gamera_no_grid *g,
+                                const size_t lower[3], const size_t upper[3], double dt,
+                                double gamma, double rf, double pf, double c,
+                                double low_threshold, double low_sound, size_t *low_count,
+                                size_t *hot_count, double *max_sound, double *max_pressure) {
+  if (!s || !g || !lower || !upper || !s->conserved || !(dt > 0.0) || !(gamma > 1.0) ||
+      !(rf > 0.0) || !(pf > 0.0) || !(c > 0.0) || !(low_threshold > 0.0) ||
+      !(low_sound >= 0.0))
+    return -1;
+  size_t low = 0, hot = 0;
+  double ms = 0.0, mp = 0.0;
+  int failed = 0;
+  for (size_t i = lower[0]; i < upper[0]; ++i)
+    for (size_t j = lower[1]; j < upper[1]; ++j)
+      for (size_t k = lower[2]; k < upper[2]; ++k) {
+        const size_t cell = idx3(s->cell_extent, i, j, k);
+        double *u = &s->conserved[cell * 5];
+        prim p;
+        if (s_c2p(u, gamma, rf, pf, &p) != 0) {
+          failed = 1;
+          continue;
+        }
+        int changed = 0;
+        if (p.density <= low_threshold) {
+          p.pressure = fmax(pf, p.density * low_sound * low_sound / gamma);
+          ++low;
+          changed = 1;
+        }
+        const double cs = sqrt(gamma * p.pressure / p.density);
+        ms = fmax(ms, cs);
+        mp = fmax(mp, p.pressure);
+        if (cs > 1.5 * c) {
+          const v3 x = g->cell[cell].centroid;
+          const double r2 = x.value[0] * x.value[0] + x.value[1] * x.value[1] +
+                            x.value[2] * x.value[2];
+          const double q2 = x.value[0] * x.value[0] + x.value[1] * x.value[1];
+          if (!(r2 > 0.0) || !(q2 > DBL_MIN)) {
+            failed = 1;
+            continue;
+          }
+          const double L = sqrt(r2) * r2 / q2;
+          const double target = p.density * (1.5 * c) * (1.5 * c) / gamma;
+          p.pressure -= (dt / (L / cs)) * (p.pressure - target);
+          ++hot;
+          changed = 1;
+        }
+        if (changed && s_p2c(&p, gamma, rf, pf, u) != 0) failed = 1;
+      }
+  if (low_count) *low_count = low;
+  if (hot_count) *hot_count = hot;
+  if (max_sound) *max_sound = ms;
+  if (max_pressure) *max_pressure = mp;
+  return failed ? -1 : 0;
+}
+
 /* nonorthogonal_state.c:122-159 */
 static int s_predict(const double uo[5], const double uc[5], double r, double g,
                      double rf, double pf, double out[5]) {

@@ -72,6 +72,13 @@ int gcso_local_timestep(const gamera_no_grid *grid, const double *conserved,
                         const gamera_no_timestep_options *options,
                         const gamera_no_vec3 *background_cell, double *dt);
 
+int gcso_apply_pressure_control(gamera_no_storage *storage, const gamera_no_grid *grid,
+                                const size_t lower[3], const size_t upper[3], double dt,
+                                double gamma, double density_floor, double pressure_floor,
+                                double light_speed, double low_density_threshold,
+                                double low_density_sound_speed, size_t *low_count,
+                                size_t *hot_count, double *max_sound, double *max_pressure);
+
 int gcso_mi_apply_constant_pedersen(const gamera_mi_solver_config *config,
                                     const double *potential, double *result);
 int gcso_mi_solve_constant_pedersen(const gamera_mi_solver_config *config,

@@ -63,6 +63,11 @@ def lib():
                 ("gcso_sync_faces", C.c_int, [P(abi.Storage), P(C.c_size_t),
                                               C.c_size_t, C.c_int]),
                 ("gcso_sync_edges", C.c_int, [C.c_void_p, P(abi.Storage)]),
+                ("gcso_apply_pressure_control", C.c_int,
+                 [P(abi.Storage), P(abi.Grid), P(C.c_size_t), P(C.c_size_t), C.c_double,
+                  C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                  C.c_double, P(C.c_size_t), P(C.c_size_t), P(C.c_double),
+                  P(C.c_double)]),
                 ("gcso_mi_apply_constant_pedersen", C.c_int,
                  [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double)]),
                 ("gcso_mi_solve_constant_pedersen", C.c_int,

@@ -44,6 +44,11 @@ def _bind_common(lib):
             C.c_int, [C.c_void_p, P(abi.Grid), P(abi.Storage)]),
         "gamera_cs_fill_magnetic_face_halos_planned": (
             C.c_int, [C.c_void_p, P(abi.Grid), P(abi.Storage)]),
+        "gamera_no_apply_pressure_control": (
+            C.c_int, [P(abi.Storage), P(abi.Grid), P(C.c_size_t), P(C.c_size_t),
+                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                      C.c_double, C.c_double, P(C.c_size_t), P(C.c_size_t),
+                      P(C.c_double), P(C.c_double)]),
         "gamera_mi_solve_constant_pedersen": (
             C.c_int, [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double),
                       P(abi.MiSolverStats)]),

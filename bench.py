@@ -488,7 +488,7 @@ def run_earth(lib, torch, device, args, dist, ctx):
                 "arguments": "gamma 5/3, floors 1e-6/1e-8, c 10, low density 1e-3, "
                              "low-density sound speed 1e-7",
                 "low_density_cells": pc_low.value, "high_sound_speed_cells": pc_hot.value,
-                "gpu_launches_per_step": 24 + 18 + 2}}
+                "gpu_launches_per_step": 24 + 18 + 1}}
 
 
 ENS_SEED = 2024

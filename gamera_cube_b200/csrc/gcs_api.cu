@@ -290,9 +290,8 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   }
   if (post_control) {
     // the Earth drivers' post-step pressure control with this step's dt,
-    // then the CFL step of the controlled state
-    gcs::launch_pressure_control(C, C.pc, 0.0, true, s);
-    gcs::launch_timestep(X, O, s);
+    // fused with the CFL reduction of the controlled state
+    gcs::launch_pressure_control(C, C.pc, 0.0, &O, s);
   }
   if (driver_mode) {
     gcs::launch_count_step(X, s);

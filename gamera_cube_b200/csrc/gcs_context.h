@@ -124,8 +124,10 @@ struct Context {
 // gcs_pressure.cu
 int pressure_prepare(Context &C, const gamera_no_grid *grid);
 int pressure_reset_async(Context &C);
+// cfl set (the driver loop): dt from the step parameters, failures into the
+// step status, and the CFL step of the controlled state reduced with it.
 void launch_pressure_control(Context &C, const PressureControl &pc, double dt,
-                             bool from_params, cudaStream_t s);
+                             const Opts *cfl, cudaStream_t s);
 
 }  // namespace gcs
 

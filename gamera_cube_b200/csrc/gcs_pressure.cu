@@ -45,19 +45,58 @@ __device__ inline unsigned long long warp_max(unsigned long long v) {
   return v;
 }
 
+// CFL candidate of one active cell (nonorthogonal_step.c:449-525, the same
+// arithmetic as the recovery kernel's fused CFL reduction): false when the
+// reference fails the cell.
+__device__ inline bool cfl_candidate(const double u[5], const double bn[3], const double *b0,
+                                     double cflmin, const Opts &O, double *cand) {
+  Prim p;
+  if (cons_to_prim(u, O.t_gamma, O.t_rho_floor, O.t_p_floor, &p)) return false;
+  const double cs = sqrt(O.t_gamma * p.p / p.rho);
+  double va = 0.0;
+  if (O.t_mhd) {
+    double bx = bn[0], by = bn[1], bz = bn[2];
+    if (b0) {
+      bx = bn[0] + b0[0];
+      by = bn[1] + b0[1];
+      bz = bn[2] + b0[2];
+    }
+    double s2 = 0.0;
+    s2 += bx * bx;
+    s2 += by * by;
+    s2 += bz * bz;
+    va = sqrt(s2) / sqrt(p.rho);
+    if (O.t_boris) va = O.t_c * va / hypot(O.t_c, va);
+  }
+  double v2 = 0.0;
+  v2 += p.vx * p.vx;
+  v2 += p.vy * p.vy;
+  v2 += p.vz * p.vz;
+  const double speed = sqrt(v2) + hypot(cs, va);
+  const double c0 = O.t_cfl * cflmin / speed;
+  if (!isfinite(c0) || c0 <= 0.0) return false;
+  *cand = c0;
+  return true;
+}
+
 // nonorthogonal_step.c:95-152, one thread per active cell; dt from the step
-// parameters when prm is set (the device driver loop), else `dt`.
+// parameters when prm is set (the device driver loop), else `dt`.  In the
+// driver loop (with_cfl) the kernel also reduces the CFL step of the
+// controlled state into the status word, the next step's dt.
 __global__ void __launch_bounds__(256) k_pressure_control(
-    Dims D, DevState S, const double *dipole_l, PressureControl pc, double dt,
-    const StepParams *prm, PcStats *out, DevStatus *status) {
-  const long long count = (long long)D.nr * D.n * D.n;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    Dims D, DevState S, DevGeom G, DevBg BG, Opts O, const double *dipole_l,
+    PressureControl pc, double dt, const StepParams *prm, PcStats *out, DevStatus *status,
+    int with_cfl) {
+  const int count = D.nr * D.n * D.n;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
   unsigned long long low = 0, hot = 0, smax = 0, pmax = 0;
+  double cand = DBL_MAX;
   if (t < count) {
-    const int i = (int)(t / ((long long)D.n * D.n));
-    const int j = (int)((t / D.n) % D.n);
-    const int k = (int)(t % D.n);
+    const int nn = D.n * D.n;
+    const int i = t / nn;
+    const int j = (t - i * nn) / D.n;
+    const int k = t - i * nn - j * D.n;
     const long long c = f * D.Nn + D.node(D.g + i, D.g + j, D.g + k);
     if (prm) dt = prm->dt;
     double u[5];
@@ -91,26 +130,46 @@ __global__ void __launch_bounds__(256) k_pressure_control(
       }
       if (!bad && changed) {
         double w[5];
-        if (prim_to_cons(p, pc.gamma, pc.density_floor, pc.pressure_floor, w) != 0)
+        if (prim_to_cons(p, pc.gamma, pc.density_floor, pc.pressure_floor, w) != 0) {
           bad = true;
-        else
-          for (int m = 0; m < 5; ++m) S.U[m][c] = w[m];
+        } else {
+          for (int m = 0; m < 5; ++m) {
+            S.U[m][c] = w[m];
+            u[m] = w[m];
+          }
+        }
       }
     }
     if (bad) {
       atomicOr(&out->failed, 1);
       if (status) fail(status, kStagePressureControl, 0, f, D.g + i, D.g + j, D.g + k);
     }
+    if (with_cfl) {
+      // the cell as stored now: controlled, or unchanged
+      const double bn[3] = {S.B[0][c], S.B[1][c], S.B[2][c]};
+      double b0[3];
+      if (O.t_bg)
+        for (int m = 0; m < 3; ++m) b0[m] = BG.b0[m][c];
+      if (!cfl_candidate(u, bn, O.t_bg ? b0 : nullptr, G.cflmin[c], O, &cand)) {
+        cand = DBL_MAX;
+        fail(status, kStageTimestep, 0, f, D.g + i, D.g + j, D.g + k);
+      }
+    }
   }
   low = warp_sum(low);
   hot = warp_sum(hot);
   smax = warp_max(smax);
   pmax = warp_max(pmax);
+  if (with_cfl)
+    for (int o = 16; o > 0; o >>= 1) cand = fmin(cand, __shfl_xor_sync(0xffffffffu, cand, o));
   if ((threadIdx.x & 31) == 0) {
     if (low) atomicAdd(&out->low, low);
     if (hot) atomicAdd(&out->hot, hot);
     if (smax) atomicMax(&out->max_sound_bits, smax);
     if (pmax) atomicMax(&out->max_pressure_bits, pmax);
+    // positive doubles order as unsigned 64-bit integers
+    if (with_cfl && cand < DBL_MAX)
+      atomicMin(&status->cfl_min_bits, (unsigned long long)__double_as_longlong(cand));
   }
 }
 
@@ -180,12 +239,14 @@ int pressure_reset_async(Context &C) {
 }
 
 void launch_pressure_control(Context &C, const PressureControl &pc, double dt,
-                             bool from_params, cudaStream_t s) {
+                             const Opts *cfl, cudaStream_t s) {
   const Dims &D = C.X.D;
   const long long count = (long long)D.nr * D.n * D.n;
+  const Opts none{};
   k_pressure_control<<<dim3((unsigned)((count + 255) / 256), kFaces), 256, 0, s>>>(
-      D, C.X.S, C.pc_dipole, pc, dt, from_params ? C.X.params : nullptr,
-      (PcStats *)C.pc_stats, from_params ? C.X.status : nullptr);
+      D, C.X.S, C.X.G, C.X.BG, cfl ? *cfl : none, C.pc_dipole, pc, dt,
+      cfl ? C.X.params : nullptr, (PcStats *)C.pc_stats, cfl ? C.X.status : nullptr,
+      cfl ? 1 : 0);
 }
 
 int pressure_read(Context &C, size_t *low, size_t *hot, double *max_sound,
@@ -221,7 +282,7 @@ int gcs_context_pressure_control(gcs_context *ctx, const gamera_no_grid *grid, d
   if (!gcs::pressure_valid(pc)) return -1;
   gcs::Context &C = ctx->c;
   if (gcs::pressure_prepare(C, grid) != 0 || gcs::pressure_reset_async(C) != 0) return -1;
-  gcs::launch_pressure_control(C, pc, dt, false, C.stream);
+  gcs::launch_pressure_control(C, pc, dt, nullptr, C.stream);
   if (cudaGetLastError() != cudaSuccess) return -1;
   int failed = 0;
   if (gcs::pressure_read(C, low_density_cell_count, high_sound_speed_cell_count,

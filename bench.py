@@ -52,6 +52,15 @@ FLUX_BYTES_PER_FACE = 33 * 8
 # central8 area sums (2), length (1), B0 projections (2), edge density
 # cells (1), written EMF (1): 25 doubles (each counted once per edge).
 EMF_BYTES_PER_EDGE = 25 * 8
+# Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per
+# face of a flux launch and per edge of an edge-EMF launch: the mean of the
+# three launches of each sweep in the ncu capture summarised in
+# profiles/k_flux_full_32x32x48.md (6 x 32x32x48, state arrays larger than
+# L2), divided by the faces or edges one launch processes there.  The
+# sweeps stream their arrays, so the traffic of a launch of the bench's
+# workload is these figures times its faces or edges.
+FLUX_TRAFFIC_BYTES_PER_FACE = 354.5
+EMF_TRAFFIC_BYTES_PER_EDGE = 259.4
 
 
 def peaks():
@@ -253,6 +262,11 @@ def run_gpu(args):
         alg = 3 * edges_per_dir * EMF_BYTES_PER_EDGE
     else:
         alg = cells * STEP_BYTES_PER_CELL
+    traffic = None
+    if dom == "flux":
+        traffic = faces_per_dir * FLUX_TRAFFIC_BYTES_PER_FACE
+    elif dom == "edge_emf":
+        traffic = edges_per_dir * EMF_TRAFFIC_BYTES_PER_EDGE
     per_launch_ms = stages[dom] / 3.0 if dom in ("flux", "edge_emf") else stages[dom]
     hbm, peak_kind = peaks()
     achieved = (alg / 3.0 if dom in ("flux", "edge_emf") else alg) / (
@@ -338,7 +352,12 @@ def run_gpu(args):
                          "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6650 GB/s",
-                         "traffic": None,
+                         "traffic": traffic,
+                         "traffic_source": None if traffic is None else
+                         "ncu DRAM bytes per launch of the 6x32x32x48 capture, scaled "
+                         "by faces/edges per launch (profiles/k_flux_full_32x32x48.md)",
+                         "algorithmic_bytes_per_launch": alg / 3.0
+                         if dom in ("flux", "edge_emf") else alg,
                          "step_share": stages[dom] / step_ms_prof,
                          "step_hbm_frac": cells * STEP_BYTES_PER_CELL /
                          (ms_local / args.steps * 1e-3) / 1e9 / hbm},

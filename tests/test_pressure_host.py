@@ -75,3 +75,17 @@ def test_oracle_rejects_invalid_arguments():
         assert fn(C.byref(case.storage[0]), C.byref(case.grid[0]), lo, hi, dt, gamma,
                   pu.RHO_FLOOR, pu.P_FLOOR, c, thr, cs, None, None, None, None) == -1
     np.testing.assert_array_equal(case.arrays(0)["conserved"], before)
+
+
+def test_c_abi_rejects_missing_handles():
+    """Host-side argument checks of the device entry points (no CUDA call is
+    reached): a missing context, configuration or plan is -1."""
+    import gamera_cube_b200
+    from gamera_cube_b200 import abi
+    lib = gamera_cube_b200.lib
+    cfg = abi.PressureControl(pu.GAMMA, pu.RHO_FLOOR, pu.P_FLOOR, 10.0, 1e-3, 1e-7)
+    assert lib.gcs_context_pressure_control(None, None, 0.1, C.byref(cfg), None, None,
+                                            None, None) == -1
+    assert lib.gcs_context_set_pressure_control(None, None, C.byref(cfg)) == -1
+    assert lib.gcs_context_pressure_control_stats(None, None, None, None, None, 0) == -1
+    assert lib.gcs_mi_tensor_plan_set_ordering(None, 1) == -1

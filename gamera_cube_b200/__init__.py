@@ -1,8 +1,11 @@
 """Python host interface of libgamera_cs_b200 (the B200 cubed-sphere MHD
 step and ionosphere solve).
 
-The shared library is built in place (``make -C gamera_cube_b200``); importing
-this package loads it and raises if it is missing: there is no CPU fallback.
+The shared library is built in place (``make -C gamera_cube_b200``).  It is
+loaded on first use of ``gamera_cube_b200.lib`` (so the ctypes struct mirrors
+in ``abi`` and the case descriptions in ``cases`` can be imported without
+it), and that first use raises if the library is missing: there is no CPU
+fallback.
 """
 import ctypes as C
 import os
@@ -155,6 +158,17 @@ def _load(path=None):
     return abi.bind(lib, sig)
 
 
-lib = _load()
+_lib = None
+
+
+def __getattr__(name):
+    # the library is loaded by the first access to gamera_cube_b200.lib
+    global _lib
+    if name == "lib":
+        if _lib is None:
+            _lib = _load()
+        return _lib
+    raise AttributeError("module %r has no attribute %r" % (__name__, name))
+
 
 __all__ = ["abi", "lib", "LIBRARY_PATH"]

@@ -11,17 +11,23 @@
 // file-scope array below, sized once for the largest supported call.
 //
 // The array occupies kScratchBytes of every GPU that loads this library
-// until the process exits.  All calls share it and it keeps the contents of
-// the last call; every slot a call reads is written earlier in the same
-// call, so nothing has to be cleared between calls.  Calls that overlap on
-// the GPU (from several host threads or streams) race on the array and must
-// be serialised by the caller.
+// until the process exits.  With CUDA's default lazy module loading the
+// library's device code, and this array with it, is loaded onto a device by
+// the first call there of any entry point that touches device code; a
+// caller that must fix its footprint at start-up makes one call of this
+// entry point then (or runs with CUDA_MODULE_LOADING=EAGER).  Later calls
+// change the device memory footprint by nothing.
+//
+// All calls share the array and it keeps the contents of the last call;
+// every slot a call reads is written earlier in the same call, so nothing
+// has to be cleared between calls.  Calls that overlap on the GPU (from
+// several host threads or streams) race on the array and must be
+// serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "gamera_cs_b200.h"
 #include "gcs_physics.cuh"
@@ -31,7 +37,6 @@ namespace {
 constexpr int kBlock = 256;                // cells per block
 constexpr int kMaxBlocks = 65536;          // partial minima
 constexpr long long kMaxCells = (long long)kBlock * kMaxBlocks;  // 16,777,216
-constexpr int kMaxDevices = 64;
 
 // Scratch layout: kMaxBlocks partial minima, kMaxBlocks failure flags,
 // then the reduced minimum and its failure flag.
@@ -44,9 +49,6 @@ struct Scratch {
 constexpr size_t kScratchBytes = sizeof(Scratch);
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
-
-std::mutex g_setup_mutex;
-Scratch *g_scratch_ptr[kMaxDevices] = {};
 
 thread_local char g_error[256] = "";
 
@@ -164,27 +166,26 @@ __global__ void k_final(Scratch *s, int blocks) {
   }
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device with that device current (the array's host-side name is only a
-// stand-in and must never be passed to a kernel).
+// Device address of the scratch array in the current context of the current
+// device.  The array's host-side name is only a stand-in and must never be
+// passed to a kernel.  The address is looked up on every call rather than
+// cached: after cudaDeviceReset, or with another context current on the
+// device (a driver-API caller), the module is loaded anew and an address
+// kept from before would be stale.
 Scratch *scratch_for_current_device() {
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
     snprintf(g_error, sizeof(g_error), "no current CUDA device");
     return nullptr;
   }
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (g_scratch_ptr[dev] == nullptr) {
-    void *ptr = nullptr;
-    const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_scratch);
-    if (rc != cudaSuccess || ptr == nullptr) {
-      snprintf(g_error, sizeof(g_error), "cudaGetSymbolAddress failed: %s",
-               cudaGetErrorString(rc));
-      return nullptr;
-    }
-    g_scratch_ptr[dev] = (Scratch *)ptr;
+  void *ptr = nullptr;
+  const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_scratch);
+  if (rc != cudaSuccess || ptr == nullptr) {
+    snprintf(g_error, sizeof(g_error), "cudaGetSymbolAddress failed: %s",
+             cudaGetErrorString(rc));
+    return nullptr;
   }
-  return g_scratch_ptr[dev];
+  return (Scratch *)ptr;
 }
 
 }  // namespace
@@ -223,16 +224,26 @@ int gcs_local_timestep_noalloc(const size_t cell_extent[3],
       snprintf(g_error, sizeof(g_error), "invalid active range");
       return -1;
     }
-    n[a] = (long long)(active_upper[a] - active_lower[a]);
+    // each axis is checked on its own first, so the product below cannot
+    // overflow
+    const size_t na = active_upper[a] - active_lower[a];
+    if (na > (size_t)kMaxCells) {
+      snprintf(g_error, sizeof(g_error),
+               "gcs_local_timestep_noalloc: %zu active cells along axis %d exceed "
+               "the maximum of %lld per call",
+               na, a, kMaxCells);
+      return -1;
+    }
+    n[a] = (long long)na;
   }
-  const long long count = n[0] * n[1] * n[2];
-  if (count > kMaxCells) {
+  if (n[0] * n[1] > kMaxCells || n[0] * n[1] * n[2] > kMaxCells) {
     snprintf(g_error, sizeof(g_error),
-             "gcs_local_timestep_noalloc: %lld active cells exceed the maximum "
-             "of %lld per call",
-             count, kMaxCells);
+             "gcs_local_timestep_noalloc: %lld x %lld x %lld active cells exceed "
+             "the maximum of %lld per call",
+             n[0], n[1], n[2], kMaxCells);
     return -1;
   }
+  const long long count = n[0] * n[1] * n[2];
   Scratch *s = scratch_for_current_device();
   if (s == nullptr) return -1;
   const int blocks = (int)((count + kBlock - 1) / kBlock);
@@ -242,7 +253,17 @@ int gcs_local_timestep_noalloc(const size_t cell_extent[3],
                                 (long long)active_lower[0],
                                 (long long)active_lower[1],
                                 (long long)active_lower[2], n[1], n[2], count, o);
-  k_final<<<1, 1024>>>(s, blocks);
+  cudaError_t launch = cudaGetLastError();
+  if (launch == cudaSuccess) {
+    k_final<<<1, 1024>>>(s, blocks);
+    launch = cudaGetLastError();
+  }
+  if (launch != cudaSuccess) {
+    // a failed launch leaves the array holding an earlier call's result
+    snprintf(g_error, sizeof(g_error), "kernel launch failed: %s",
+             cudaGetErrorString(launch));
+    return -1;
+  }
   double result = 0.0;
   int failed = 1;
   if (cudaMemcpy(&result, &s->result, sizeof(double), cudaMemcpyDeviceToHost) !=

@@ -338,11 +338,16 @@ size_t gcs_context_device_bytes(const gcs_context *ctx);
  * device array of gcs_noalloc_scratch_bytes() bytes (about 768 KiB) that
  * every GPU loading this library holds until exit.  At most 16,777,216
  * active cells per call; larger boxes are rejected with -1 and a message in
- * gcs_noalloc_last_error().  The first call on each device looks up the
- * array's device address, so make it before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race and must be
- * serialised.  Runs on the default stream and returns after the result is
- * on the host. */
+ * gcs_noalloc_last_error().  Every call looks up the array's device
+ * address in the current context (an address kept from before a
+ * cudaDeviceReset would be stale), so make calls outside stream capture.
+ * Under CUDA's default lazy module loading the array is loaded onto a
+ * device by the first call there: a caller that must fix its footprint at
+ * start-up makes one call then (or sets CUDA_MODULE_LOADING=EAGER); later
+ * calls change the device footprint by nothing.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised.  A failed
+ * kernel launch returns -1.  Runs on the default stream and returns after
+ * the result is on the host. */
 int gcs_local_timestep_noalloc(const size_t cell_extent[3],
                                const gamera_no_cell_geometry *cells,
                                const double *conserved,

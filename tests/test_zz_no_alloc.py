@@ -86,14 +86,21 @@ def test_noalloc_timestep_matches_context_entry_point(lib):
         assert lib.gcs_context_upload_background(ctx, case.background) == 0
         assert lib.gcs_context_upload_state(ctx, case.storage) == 0
         inputs = [_face_inputs(case, f) for f in range(6)]
+        torch.cuda.synchronize()
+        free = []
         for call in range(2):       # two calls in a row share the scratch
             want = C.c_double()
             assert lib.gcs_context_timestep(ctx, case.timestep_options,
                                             C.byref(want)) == 0
             got = _noalloc_min(lib, case, inputs)
+            free.append(torch.cuda.mem_get_info()[0])
             assert abs(got - want.value) <= RTOL * want.value, (call, got,
                                                                want.value)
             assert abs(got - case.local_timestep()) <= RTOL * got
+        # once the library is loaded, a call changes the device footprint
+        # by nothing
+        got = _noalloc_min(lib, case, inputs)
+        assert torch.cuda.mem_get_info()[0] == free[-1], (free, got)
         assert 0 < lib.gcs_noalloc_scratch_bytes() < 1 << 20
     finally:
         lib.gcs_context_destroy(ctx)

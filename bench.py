@@ -21,8 +21,11 @@ constant Pedersen, rel. residual 1e-8): ms per call on the device, end to
 end through the drop-in, and the reference's single-thread CPU solve.
 
 --impl reference times the reference's own CPU step (oracle/_ref, the
-unmodified reference library, all host threads) on a bounded sample of the
-same workload.
+unmodified reference library built from its sources, OpenMP on every
+physical host core) on the same workload: the same 6 x 96x96x192 case built
+through the reference's own set-up API, 1 warm-up step and a bounded number
+of timed steps (--ref-steps).  That process loads no library of this
+repository.
 """
 import argparse
 import ctypes as C
@@ -54,11 +57,10 @@ FLUX_BYTES_PER_FACE = 33 * 8
 EMF_BYTES_PER_EDGE = 25 * 8
 # Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per
 # face of a flux launch and per edge of an edge-EMF launch: the mean of the
-# three launches of each sweep in the ncu capture summarised in
-# profiles/k_flux_full_32x32x48.md (6 x 32x32x48, state arrays larger than
-# L2), divided by the faces or edges one launch processes there.  The
-# sweeps stream their arrays, so the traffic of a launch of the bench's
-# workload is these figures times its faces or edges.
+# three launches of each sweep in an ncu capture of the 6 x 32x32x48 case
+# (state arrays larger than L2), divided by the faces or edges one launch
+# processes there.  The sweeps stream their arrays, so the traffic of a
+# launch of the bench's workload is these figures times its faces or edges.
 FLUX_TRAFFIC_BYTES_PER_FACE = 354.5
 EMF_TRAFFIC_BYTES_PER_EDGE = 259.4
 
@@ -126,6 +128,30 @@ class ClockSampler:
                           if r[3 + q].lower().startswith("active")})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def physical_cores():
+    try:
+        import psutil
+        n = psutil.cpu_count(logical=False)
+        if n:
+            return int(n)
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def spawn_ranks(n_gpus):
+    """--gpus N without a torchrun environment: start N ranks (one per GPU)
+    through torch.distributed.run on 127.0.0.1 and return its exit code."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(n_gpus), "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
 
 
 def dist_init(n_gpus):
@@ -294,6 +320,27 @@ def run_gpu(args):
     barrier(dist, device)
     e2e_value = total_cells * e2e_steps / e2e_s
 
+    # the same drop-in call in resident mode: the device copy of the state
+    # stays authoritative between calls (uploaded by the first call), each
+    # call uploads its step parameters and reads back the step status
+    if lib.gcs_context_set_resident(ctx, 1) != 0:
+        raise RuntimeError("resident mode rejected")
+    if lib.gcs_context_advance_host(ctx, hs.storage, C.byref(opts), 0.5, dtv.value) != 0:
+        raise RuntimeError("drop-in step failed")
+    res_steps = max(1, min(args.steps, 10))
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    t1 = time.perf_counter()
+    for _ in range(res_steps):
+        if lib.gcs_context_advance_host(ctx, hs.storage, C.byref(opts), 0.5,
+                                        dtv.value) != 0:
+            raise RuntimeError("resident drop-in step failed")
+    torch.cuda.synchronize(device)
+    res_s = max_over_ranks(time.perf_counter() - t1, dist, device)
+    barrier(dist, device)
+    lib.gcs_context_set_resident(ctx, 0)
+    e2e_resident = total_cells * res_steps / res_s
+
     mi_solo = run_mi(lib, torch, device, args.mi_solves) if args.mi_solves > 0 else None
     bulk = run_bulk(lib, torch, device, args, dist) if args.bulk else None
     earth = run_earth(lib, torch, device, args, dist, ctx) if args.earth_steps > 0 else None
@@ -324,8 +371,7 @@ def run_gpu(args):
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic (seeded solar wind + dipole, built on the device)",
-            "config": {"workload": "cubed-sphere 6 x %dx%dx%d FP64 MHD step, "
-                                   "solar wind + aligned dipole" % (n, n, nr),
+            "config": {"workload": workload_name(nr, n),
                        "faces": 6, "angular": n, "radial": nr,
                        "cells_per_gpu": cells, "ghost": 4,
                        "graph": "one CUDA graph per step, device-side dt",
@@ -346,7 +392,14 @@ def run_gpu(args):
                     "h2d_bytes_per_step": hs.bytes_state,
                     "d2h_bytes_per_step": hs.bytes_state,
                     "call": "gcs_context_advance_host (drop-in step, pinned host "
-                            "buffers, %d steps)" % e2e_steps},
+                            "buffers, %d steps)" % e2e_steps,
+                    "resident": {"value": e2e_resident, "unit": "cell-updates/s",
+                                 "steps": res_steps,
+                                 "h2d_bytes_per_step": 56, "d2h_bytes_per_step": 120,
+                                 "call": "the same drop-in call in resident mode "
+                                         "(gcs_context_set_resident): step parameters "
+                                         "up, step status down, state kept on the "
+                                         "device"}},
             "roofline": {"bound": "hbm", "kernel": dom,
                          "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm,
@@ -354,8 +407,8 @@ def run_gpu(args):
                          if peak_kind == "measured" else "fallback 6650 GB/s",
                          "traffic": traffic,
                          "traffic_source": None if traffic is None else
-                         "ncu DRAM bytes per launch of the 6x32x32x48 capture, scaled "
-                         "by faces/edges per launch (profiles/k_flux_full_32x32x48.md)",
+                         "ncu DRAM bytes per launch of a 6x32x32x48 capture, scaled "
+                         "by faces/edges per launch",
                          "algorithmic_bytes_per_launch": alg / 3.0
                          if dom in ("flux", "edge_emf") else alg,
                          "step_share": stages[dom] / step_ms_prof,
@@ -823,25 +876,35 @@ def _ref_bench_path():
     return os.path.join(REPO, "oracle", "_ref", "ref_bench")
 
 
-def cpu_baseline(args, steps=None):
+def ref_bench(nr, n, warmup, steps, seed=1000):
+    """The unmodified reference step (oracle/_ref/ref_bench: the case built by
+    the reference's set-up API, then the Earth driver's dt rule and one
+    planned six-face step per iteration, only the step loop timed), OpenMP
+    on every physical core.  Returns its JSON record."""
+    cores = physical_cores()
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close",
+               OMP_PLACES="cores")
+    out = subprocess.run([_ref_bench_path(), "2", str(nr), str(n), str(warmup),
+                          str(steps), str(seed)],
+                         capture_output=True, text=True, env=env, timeout=3000)
+    if out.returncode != 0:
+        raise RuntimeError("reference CPU run failed: " + out.stderr[-500:])
+    rec = json.loads(out.stdout.strip().splitlines()[-1])
+    rec["cores"] = cores
+    return rec
+
+
+def cpu_baseline(args):
     """The reference's own CPU step on a bounded sample of the workload (the
-    same case at 48 radial x 16 x 16 angular cells per face), all host
-    threads; falls back to the CPU restatement (one thread) if the
-    reference library was not built."""
-    nr, n = args.cpu_nr, args.cpu_n
-    steps = steps or args.cpu_steps
-    exe = _ref_bench_path()
-    threads = os.cpu_count() or 1
-    if os.path.exists(exe):
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close",
-                   OMP_PLACES="cores")
-        out = subprocess.run([exe, "2", str(nr), str(n), "1", str(steps), "1000"],
-                             capture_output=True, text=True, env=env, timeout=900)
-        if out.returncode != 0:
-            raise RuntimeError("reference CPU run failed: " + out.stderr[-500:])
-        rec = json.loads(out.stdout.strip().splitlines()[-1])
+    same case at 48 radial x 32 x 32 angular cells per face: set-up about
+    10 s and 3 timed steps), all physical cores; falls back to the CPU
+    restatement (one thread) if the reference library was not built."""
+    nr, n, steps = args.cpu_nr, args.cpu_n, args.cpu_steps
+    if os.path.exists(_ref_bench_path()):
+        rec = ref_bench(nr, n, 1, steps)
         return {"value": rec["cell_updates_per_s"], "unit": "cell-updates/s",
-                "cores": rec["threads"], "kind": "reference",
+                "cores": rec["cores"], "threads": rec["threads"],
+                "kind": "reference",
                 "sample": "reference CPU step (OpenMP), 6 x %dx%dx%d wind+dipole "
                           "case, %d timed steps after 1 warm-up" % (n, n, nr, steps)}
     from oracle import oracle_cases
@@ -853,28 +916,48 @@ def cpu_baseline(args, steps=None):
         case.step(0.5, dt)
     sec = time.perf_counter() - t
     return {"value": 6 * nr * n * n * steps / sec, "unit": "cell-updates/s",
-            "cores": 1, "kind": "port",
+            "cores": 1, "threads": 1, "kind": "port",
             "sample": "CPU restatement, 6 x %dx%dx%d wind+dipole case, %d steps"
                       % (n, n, nr, steps)}
 
 
+def workload_name(nr, n):
+    return ("cubed-sphere 6 x %dx%dx%d FP64 MHD step, solar wind + aligned dipole"
+            % (n, n, nr))
+
+
 def run_reference(args):
+    """The reference arm: rank 0 times the reference's own CPU step on this
+    bench's workload (same sizes and case), the other ranks exit."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    steps = max(1, args.steps)
-    base = cpu_baseline(args, steps=min(steps, args.cpu_steps))
-    line = {"impl": "reference", "metric": METRIC, "value": base["value"],
-            "unit": base["unit"], "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "cubed-sphere 6 x %dx%dx%d FP64 MHD step, "
-                                   "solar wind + aligned dipole (bounded CPU "
-                                   "sample 6 x %dx%dx%d)" % (
-                                       args.n, args.n, args.nr, args.cpu_n,
-                                       args.cpu_n, args.cpu_nr)},
+    if not os.path.exists(_ref_bench_path()):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference library not built (make -C oracle ref)"}))
+        return
+    steps = max(1, min(args.steps, args.ref_steps))
+    rec = ref_bench(args.nr, args.n, 1, steps)
+    value = rec["cell_updates_per_s"]
+    base = {"value": value, "unit": "cell-updates/s", "cores": rec["cores"],
+            "threads": rec["threads"], "kind": "reference",
+            "sample": "reference CPU step (OpenMP, %d threads on %d physical cores, "
+                      "1 process), the full 6 x %dx%dx%d case, %d timed steps after "
+                      "1 warm-up (set-up %.0f s not timed)"
+                      % (rec["threads"], rec["cores"], args.n, args.n, args.nr, steps,
+                         rec["setup_seconds"])}
+    line = {"impl": "reference", "metric": METRIC, "value": value,
+            "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": rec["seconds"] / steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded solar wind + dipole, built by "
+                                    "the reference's set-up API)",
+            "config": {"workload": workload_name(args.nr, args.n), "faces": 6,
+                       "angular": args.n, "radial": args.nr,
+                       "cells_per_gpu": 6 * args.nr * args.n * args.n, "ghost": 4,
+                       "same_config": True},
             "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": base["unit"],
+            "e2e": {"value": value, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.mi_solves > 0:
         line["mi"] = mi_cpu_baseline()
@@ -890,8 +973,11 @@ def main():
     ap.add_argument("--nr", type=int, default=NR)
     ap.add_argument("--n", type=int, default=N)
     ap.add_argument("--cpu-nr", type=int, default=48)
-    ap.add_argument("--cpu-n", type=int, default=16)
-    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--cpu-n", type=int, default=32)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--ref-steps", type=int, default=2,
+                    help="timed reference CPU steps of the full workload "
+                         "(--impl reference)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--mi-every", type=int, default=10,
                     help="steps between ionosphere coupling updates in the "
@@ -911,6 +997,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.gpus > 1 and "RANK" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     if args.impl == "reference":
         run_reference(args)
     elif args.only_mi:

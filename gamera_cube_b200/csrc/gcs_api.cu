@@ -37,11 +37,14 @@ bool same_value(double a, double b) {
   return std::isfinite(a) && std::isfinite(b) && fabs(a - b) <= 8e-15 * scale;
 }
 
+// Stage names of the MHD_FAILURE line.  The three B recoveries (predictor,
+// update, final) keep separate codes in gcs_context_failure but print the
+// reference's one name for its recovery, recover_B (nonorthogonal_step.c:351).
 const char *kStageNames[] = {
-    "none",           "predict",         "recover_predict", "reconstruct_face",
+    "none",           "predict",         "recover_B",       "reconstruct_face",
     "kinetic_fluid",  "kinetic_maxwell", "emergency",       "edge_geometry",
     "edge_velocity",  "transverse_field", "edge_density",   "compute_edge_emf",
-    "boris_after_hydro", "recover_update", "recover_B",     "timestep",
+    "boris_after_hydro", "recover_B",    "recover_B",       "timestep",
     "host_callback",  "solve_edge_field", "options",        "pressure_control"};
 
 // Option checks of the reference step and of each stage it calls

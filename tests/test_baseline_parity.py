@@ -1,0 +1,336 @@
+"""GPU parity of the plain FP64 step at the benchmark's own sizes, and the
+step's failure path under poisoned input.
+
+Configuration C1 (6 faces x 32 x 32 angular x 48 radial, solar wind + aligned
+dipole, seeded +-1 % density noise, log-stretched r in [2.5, 30]) is built
+by the compiled reference's own set-up API (oracle/_ref), three times with
+identical inputs.  The reference advances one copy with the reference Earth
+driver's dt rule (test_cubedsphere_dipole_background.c:593-670:
+dt = min(0.5 * CFL step, 1.25 * dt_prev), predictor ratio 0.5 dt / dt_prev,
+0 on the first step) for 100 steps.  Through the drop-in entry point
+gamera_cs_advance_six_with_background_planned this library advances
+
+* a second copy that is reset to the reference's state after every step, so
+  that every one of the 100 steps starts from identical inputs and is
+  compared at 1e-12 normwise relative per array (the plain path's target);
+* a third copy that is never reset (100 chained steps), compared at the end.
+
+Configuration C2 (6 x 96x96x192, 10.6 M cells, about 35 GB of host memory
+for the reference's arrays) runs its first two driver steps the same way.
+
+The failure tests poison one cell of a small wind case on the host (NaN
+density, negative density, infinite momentum, NaN face flux, negative total
+energy) and check the return code, the first failing stage and cell that
+the device reports against the reference's MHD_FAILURE line
+(nonorthogonal_step.c:14-33, :395), and the state left behind.
+"""
+import ctypes as C
+import os
+import re
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import refbind
+from tests.parity_util import STATE_ARRAYS, compare_state, divergence
+
+pytestmark = pytest.mark.gpu
+
+RTOL_STEP = 1e-12
+# 100 chained steps: per-step differences of ~1e-15 (device libm, FMA in the
+# sweeps) accumulate; measured on B200 well below this bound.
+RTOL_CHAINED = 1e-9
+C1 = (48, 32)             # radial, angular active cells per face
+C1_STEPS = 100
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import gamera_cube_b200
+    return gamera_cube_b200.lib
+
+
+@pytest.fixture(scope="module")
+def ref_lib():
+    if not refbind.ref_available():
+        pytest.skip("reference library not built (make -C oracle ref)")
+    return refbind.ref()
+
+
+def _plan(lib, case):
+    plan = C.c_void_p()
+    assert lib.gamera_cs_halo_plan_create(case.grid, case.active, case.ghost,
+                                          C.byref(plan)) == 0, lib.gcs_last_error()
+    return plan
+
+
+def _gpu_step(lib, case, plan, ratio, dt):
+    return lib.gamera_cs_advance_six_with_background_planned(
+        case.grid, case.storage, case.active, case.ghost, ratio, dt,
+        case.options, case.background, plan, None, 0.0, 0.0, None)
+
+
+def _worst(res):
+    return max(v[0] for v in res.values())
+
+
+def test_c1_hundred_driver_steps(lib, ref_lib):
+    """C1, 100 steps of the reference driver loop: every step from identical
+    inputs within 1e-12, div B at round-off, and 100 chained steps."""
+    nr, n = C1
+    ref = refbind.Case(refbind.FX_WIND, nr, n, 11)
+    synced = refbind.Case(refbind.FX_WIND, nr, n, 11)
+    chained = refbind.Case(refbind.FX_WIND, nr, n, 11)
+    p_sync, p_chain = _plan(lib, synced), _plan(lib, chained)
+    worst_step, worst_div = 0.0, 0.0
+    try:
+        dt_prev = 0.0
+        for s in range(C1_STEPS):
+            local = ref.local_timestep()
+            dt = 0.5 * local if dt_prev == 0.0 else min(0.5 * local, 1.25 * dt_prev)
+            ratio = 0.0 if dt_prev == 0.0 else 0.5 * dt / dt_prev
+            assert ref.step(ratio, dt) == 0, "reference step %d failed" % s
+            assert _gpu_step(lib, synced, p_sync, ratio, dt) == 0, \
+                "device step %d failed" % s
+            assert _gpu_step(lib, chained, p_chain, ratio, dt) == 0, \
+                "chained device step %d failed" % s
+            res = compare_state(synced, ref)
+            bad = {k: v for k, v in res.items() if not v[0] <= RTOL_STEP}
+            assert not bad, "step %d beyond %g: %s" % (s, RTOL_STEP, bad)
+            worst_step = max(worst_step, _worst(res))
+            if s % 10 == 9 or s == C1_STEPS - 1:
+                for f in range(6):
+                    worst_div = max(worst_div, divergence(synced, f))
+            synced.copy_from(ref)           # identical inputs for the next step
+            dt_prev = dt
+        chain = compare_state(chained, ref)
+        for f in range(6):
+            assert divergence(chained, f) <= 1e-9
+        assert _worst(chain) <= RTOL_CHAINED, chain
+        assert worst_div <= 1e-9
+        print("C1 100 steps: worst per-step rel %.3e, chained rel %.3e, "
+              "max div B %.3e" % (worst_step, _worst(chain), worst_div))
+    finally:
+        lib.gamera_cs_halo_plan_destroy(p_sync)
+        lib.gamera_cs_halo_plan_destroy(p_chain)
+        for c in (ref, synced, chained):
+            c.close()
+
+
+C2 = (192, 96)
+
+
+def _snapshot(case):
+    return [{name: case.arrays(f)[name].copy() for name in STATE_ARRAYS}
+            for f in range(6)]
+
+
+def _restore(case, snap):
+    for f in range(6):
+        for name in STATE_ARRAYS:
+            case.arrays(f)[name][...] = snap[f][name]
+
+
+def _compare_snapshot(case, snap):
+    worst = {}
+    for name in STATE_ARRAYS:
+        err, scale = 0.0, 0.0
+        for f in range(6):
+            a, b = case.arrays(f)[name], snap[f][name]
+            err = max(err, float(np.max(np.abs(a - b))))
+            scale = max(scale, float(np.max(np.abs(b))))
+        worst[name] = err / scale if scale > 0 else err
+    return worst
+
+
+def test_c2_two_steps_identical_inputs(lib, ref_lib):
+    """C2 (6 x 96x96x192, 10.6 M active cells), the production size: the
+    first two driver steps, each from identical inputs, device against the
+    compiled reference within 1e-12 normwise relative, div B at round-off.
+    One case built by the reference set-up API serves both paths (its state
+    arrays are saved before each reference step and restored for the
+    device step; grid and background are shared)."""
+    nr, n = C2
+    case = refbind.Case(refbind.FX_WIND, nr, n, 1000)
+    plan = _plan(lib, case)
+    try:
+        dt_prev = 0.0
+        for s in range(2):
+            local = case.local_timestep()
+            dt = 0.5 * local if dt_prev == 0.0 else min(0.5 * local, 1.25 * dt_prev)
+            ratio = 0.0 if dt_prev == 0.0 else 0.5 * dt / dt_prev
+            before = _snapshot(case)
+            assert case.step(ratio, dt) == 0, "reference step %d failed" % s
+            after_ref = _snapshot(case)
+            _restore(case, before)
+            del before
+            assert _gpu_step(lib, case, plan, ratio, dt) == 0, "device step %d" % s
+            worst = _compare_snapshot(case, after_ref)
+            bad = {k: v for k, v in worst.items() if not v <= RTOL_STEP}
+            assert not bad, "C2 step %d beyond %g: %s" % (s, RTOL_STEP, bad)
+            for f in (0, 3, 5):
+                assert divergence(case, f) <= 1e-9
+            print("C2 step %d: worst rel %.3e" % (s, max(worst.values())))
+            _restore(case, after_ref)       # the reference's state continues
+            del after_ref
+            dt_prev = dt
+    finally:
+        lib.gamera_cs_halo_plan_destroy(plan)
+        case.close()
+
+
+class _Stderr:
+    """Captures what C code writes to file descriptor 2."""
+
+    def __enter__(self):
+        self.tmp = tempfile.TemporaryFile(mode="w+b")
+        self.saved = os.dup(2)
+        os.dup2(self.tmp.fileno(), 2)
+        return self
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 2)
+        os.close(self.saved)
+        self.tmp.seek(0)
+        self.text = self.tmp.read().decode(errors="replace")
+        self.tmp.close()
+
+
+_LINE = re.compile(r"MHD_FAILURE (?:rank=\S+ )?stage=(\w+)(?: direction=(\d+))?"
+                   r"(?: face=(\d+))? local=(\d+),(\d+),(\d+)")
+
+
+def _failures(text):
+    return [(m.group(1), tuple(int(m.group(q)) for q in (4, 5, 6)),
+             None if m.group(3) is None else int(m.group(3)))
+            for m in _LINE.finditer(text)]
+
+
+def _poison(case, what, face, cell):
+    a = case.arrays(face)
+    i, j, k = cell
+    if what == "nan_density":
+        a["conserved"][i, j, k, 0] = np.nan
+    elif what == "negative_density":
+        a["conserved"][i, j, k, 0] = -1.0
+    elif what == "inf_momentum":
+        a["conserved"][i, j, k, 2] = np.inf
+    elif what == "negative_energy":
+        a["conserved"][i, j, k, 4] = -abs(a["conserved"][i, j, k, 4])
+    elif what == "nan_face_flux":
+        a["face_flux1"][i, j, k] = np.nan
+    else:
+        raise ValueError(what)
+
+
+# an active cell of face 2 at least seven cells from every seam and away
+# from the radial boundary layers, so no halo fill reads it
+_CASE = (12, 16)
+_CELL = (9, 12, 11)
+
+
+def _compare_with_nonfinite(gpu, ref):
+    """Arrays equal where non-finite (same positions, same values) and
+    within 1e-12 normwise relative on the finite entries."""
+    for name in STATE_ARRAYS:
+        worst, scale = 0.0, 0.0
+        for f in range(6):
+            a, b = gpu.arrays(f)[name], ref.arrays(f)[name]
+            fa, fb = np.isfinite(a), np.isfinite(b)
+            np.testing.assert_array_equal(fa, fb, err_msg="%s face %d" % (name, f))
+            np.testing.assert_array_equal(a[~fa], b[~fb])
+            if fa.any():
+                worst = max(worst, float(np.max(np.abs(a[fa] - b[fb]))))
+                scale = max(scale, float(np.max(np.abs(b[fb]))))
+        assert worst <= RTOL_STEP * max(scale, 1e-300), (name, worst, scale)
+
+
+def _poisoned_pair(what, face):
+    ref = refbind.Case(refbind.FX_WIND, _CASE[0], _CASE[1], 5)
+    gpu = refbind.Case(refbind.FX_WIND, _CASE[0], _CASE[1], 5)
+    dt = 0.5 * ref.local_timestep()
+    _poison(ref, what, face, _CELL)
+    _poison(gpu, what, face, _CELL)
+    return ref, gpu, dt
+
+
+@pytest.mark.parametrize("what", ["nan_density", "negative_density", "inf_momentum"])
+def test_poisoned_cell_fails_in_predictor(lib, ref_lib, what):
+    """A non-physical conserved state fails the step in the predictor on
+    both paths: rc -1, stage 'predict' at the poisoned cell, the active
+    state left as it was, and the whole state equal to the reference's
+    (both ran the seam sync and halo fills that precede the predictor)."""
+    face = 2
+    ref, gpu, dt = _poisoned_pair(what, face)
+    g0, act = gpu.ghost, gpu.active
+    act_slice = (slice(g0, g0 + act[0]), slice(g0, g0 + act[1]),
+                 slice(g0, g0 + act[2]))
+    before = {f: gpu.arrays(f)["conserved"][act_slice].copy() for f in range(6)}
+    plan = _plan(lib, gpu)
+    try:
+        with _Stderr() as r:
+            rc_ref = ref.step(0.5, dt)
+        with _Stderr() as g:
+            rc_gpu = _gpu_step(lib, gpu, plan, 0.5, dt)
+        assert rc_ref == -1 and rc_gpu == -1, (rc_ref, rc_gpu)
+        assert _failures(r.text) == [("predict", _CELL, None)], r.text
+        assert _failures(g.text) == [("predict", _CELL, face)], g.text
+        d, fc, i, j, k = (C.c_int() for _ in range(5))
+        ctx = lib.gcs_halo_plan_context(plan)
+        stage = lib.gcs_context_failure(ctx, C.byref(d), C.byref(fc), C.byref(i),
+                                        C.byref(j), C.byref(k))
+        assert stage == 1 and fc.value == face and \
+            (i.value, j.value, k.value) == _CELL
+        for f in range(6):
+            np.testing.assert_array_equal(gpu.arrays(f)["conserved"][act_slice],
+                                          before[f])
+        _compare_with_nonfinite(gpu, ref)
+    finally:
+        lib.gamera_cs_halo_plan_destroy(plan)
+        ref.close()
+        gpu.close()
+
+
+def test_poisoned_face_flux_fails(lib, ref_lib):
+    """A NaN magnetic face flux makes the predictor's B recovery fail on both
+    paths; the reference prints a recover_B line for each of the two cells
+    beside the poisoned face (nonorthogonal_step.c:351), the device reports
+    the first of them it meets, and the state left behind equals the
+    reference's."""
+    face = 4
+    ref, gpu, dt = _poisoned_pair("nan_face_flux", face)
+    plan = _plan(lib, gpu)
+    try:
+        with _Stderr() as r:
+            rc_ref = ref.step(0.5, dt)
+        with _Stderr() as g:
+            rc_gpu = _gpu_step(lib, gpu, plan, 0.5, dt)
+        assert rc_ref == -1 and rc_gpu == -1
+        i, j, k = _CELL
+        want = [("recover_B", (i, j - 1, k), None), ("recover_B", (i, j, k), None)]
+        assert sorted(_failures(r.text)) == want, r.text
+        lines = _failures(g.text)
+        assert len(lines) == 1 and lines[0][0] == "recover_B", g.text
+        assert lines[0][2] == face and lines[0][1] in ((i, j, k), (i, j - 1, k))
+        _compare_with_nonfinite(gpu, ref)
+    finally:
+        lib.gamera_cs_halo_plan_destroy(plan)
+        ref.close()
+        gpu.close()
+
+
+def test_negative_energy_is_floored_on_both_paths(lib, ref_lib):
+    """Total energy below the kinetic energy is not a failure: both paths
+    floor the pressure (nonorthogonal_state.c:60-93) and agree to 1e-12."""
+    ref, gpu, dt = _poisoned_pair("negative_energy", 2)
+    plan = _plan(lib, gpu)
+    try:
+        assert ref.step(0.0, dt) == 0
+        assert _gpu_step(lib, gpu, plan, 0.0, dt) == 0
+        res = compare_state(gpu, ref)
+        assert _worst(res) <= RTOL_STEP, res
+    finally:
+        lib.gamera_cs_halo_plan_destroy(plan)
+        ref.close()
+        gpu.close()

@@ -67,6 +67,7 @@ def _load(path=None):
         "gcs_context_reset_failure": (C.c_int, [C.c_void_p]),
         "gcs_context_stream": (C.c_size_t, [C.c_void_p]),
         "gcs_context_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+        "gcs_context_set_flux_staging": (C.c_int, [C.c_void_p, C.c_int]),
         "gcs_context_stage_times": (C.c_int, [C.c_void_p, P(C.c_double),
                                               P(C.c_longlong), C.c_int]),
         "gcs_stage_name": (C.c_char_p, [C.c_int]),

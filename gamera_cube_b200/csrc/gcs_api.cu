@@ -45,7 +45,8 @@ const char *kStageNames[] = {
     "kinetic_fluid",  "kinetic_maxwell", "emergency",       "edge_geometry",
     "edge_velocity",  "transverse_field", "edge_density",   "compute_edge_emf",
     "boris_after_hydro", "recover_B",    "recover_B",       "timestep",
-    "host_callback",  "solve_edge_field", "options",        "pressure_control"};
+    "host_callback",  "solve_edge_field", "options",        "pressure_control",
+    "tile_copy"};
 
 // Option checks of the reference step and of each stage it calls
 // (cubedsphere_step.c:23-47, nonorthogonal_sweep.c:48-62, 209-221,
@@ -1065,6 +1066,7 @@ int context_run(gcs_context *ctx, const gamera_no_advance_options *options,
     const unsigned char *b = (const unsigned char *)&O;
     for (size_t q = 0; q < sizeof(O); ++q) key = (key ^ b[q]) * 1099511628211ULL;
     key = (key ^ (unsigned long long)C.X.bulk) * 1099511628211ULL;
+    key = (key ^ (unsigned long long)(0x5354ULL + C.X.flux_staged)) * 1099511628211ULL;
     if (es) {
       const unsigned char *e = (const unsigned char *)es->dev;
       for (size_t q = 0; q < sizeof(*es->dev); ++q) key = (key ^ e[q]) * 1099511628211ULL;
@@ -1187,6 +1189,12 @@ int gcs_context_reset_failure(gcs_context *ctx) {
 
 uintptr_t gcs_context_stream(gcs_context *ctx) {
   return ctx ? (uintptr_t)ctx->c.stream : 0;
+}
+
+int gcs_context_set_flux_staging(gcs_context *ctx, int on) {
+  if (!ctx || (on != 0 && on != 1)) return -1;
+  ctx->c.X.flux_staged = on;
+  return 0;
 }
 
 int gcs_context_set_profiling(gcs_context *ctx, int on) {

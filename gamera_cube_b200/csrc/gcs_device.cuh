@@ -3,7 +3,8 @@
 // All six faces of the cube stay resident in HBM.  Every staggered array
 // (cells, the three face families, the three edge families) of a face uses
 // the same padded node index
-//     node(i, j, k) = (i * N1 + j) * N2 + k,   N_a = cell_extent[a] + 1,
+//     node(i, j, k) = (i * N1 + j) * N2 + k,   N_a = cell_extent[a] + 1
+// (N2 rounded up to a multiple of 4 so rows start on 16-byte boundaries),
 // so a cell, its three lower faces and its three lower edges share one
 // linear index and neighbours are +-1, +-N2, +-N1*N2 away.  Arrays are
 // structure-of-arrays (one double per node per component) and the six faces
@@ -159,6 +160,7 @@ enum Stage : int {
   kStageSolveEdge = 17,
   kStageOptions = 18,
   kStagePressureControl = 19,
+  kStageTileCopy = 20,   // a staged sweep's tile copy did not arrive in time
 };
 
 struct DevStatus {

@@ -488,6 +488,14 @@ void launch_timestep(const Ctx &X, const Opts &O, cudaStream_t s) {
       D, X.S, X.G, X.BG, O, 2, X.status);
 }
 
+__global__ void k_set_failure(DevStatus *st, int stage, int dir) {
+  fail(st, stage, dir, 0, 0, 0, 0);
+}
+
+void launch_set_failure(const Ctx &X, int stage, int dir, cudaStream_t s) {
+  k_set_failure<<<1, 1, 0, s>>>(X.status, stage, dir);
+}
+
 void launch_next_dt(const Ctx &X, double fraction, cudaStream_t s) {
   k_next_dt<<<1, 1, 0, s>>>(X.params, X.status, fraction);
 }

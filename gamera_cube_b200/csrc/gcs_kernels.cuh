@@ -39,6 +39,7 @@ struct Ctx {
   int n_edge_groups = 0;
   StepParams *params = nullptr;   // device
   DevStatus *status = nullptr;    // device
+  int flux_staged = 1;            // 1: TMA-staged flux sweeps (gcs_flux_tma.cuh)
   int bulk = 0;                   // 1: FP32-bulk sweeps (B32)
   int bulk_split = 0;             // radial layers [0, bulk_split) stay FP64
   Bulk<float> B32{};
@@ -59,6 +60,11 @@ void launch_flux_f64(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s
 void launch_face_velocity_f64(const Ctx &X, const Opts &O, int i0, int i1,
                               cudaStream_t s);
 void launch_edge_emf_f64(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s);
+
+// Kernel attributes and persistent grid sizes of the TMA-staged flux sweeps
+// (called at context set-up, before any stream capture).
+int prepare_flux_f64();
+int prepare_flux_f32();
 
 // FP32-bulk sweeps over the radial range [i0, i1) (gcs_kernels_bulk.cu).
 void launch_flux_f32(const Ctx &X, const Opts &O, int i0, int i1, cudaStream_t s);

@@ -17,4 +17,6 @@ void launch_edge_emf_f32(const Ctx &X, const Opts &O, int i0, int i1, cudaStream
   Sweeps<float>::edge(X, X.B32, O, i0, i1, s);
 }
 
+int prepare_flux_f32() { return prepare_flux_tma<float>(); }
+
 }  // namespace gcs

@@ -21,4 +21,6 @@ void launch_edge_emf_f64(const Ctx &X, const Opts &O, int i0, int i1, cudaStream
   Sweeps<double>::edge(X, bulk64(X), O, i0, i1, s);
 }
 
+int prepare_flux_f64() { return prepare_flux_tma<double>(); }
+
 }  // namespace gcs

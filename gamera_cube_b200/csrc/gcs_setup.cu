@@ -12,6 +12,9 @@
 #include "gcs_physics.cuh"
 #include "gcs_topology.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 namespace gcs {
 
 namespace {
@@ -443,13 +446,20 @@ int Context::allocate(const size_t active[3], size_t ghost) {
   D.E0 = D.nr + 2 * D.g;
   D.E1 = D.E2 = D.n + 2 * D.g;
   D.N1 = D.E1 + 1;
-  D.N2 = D.E2 + 1;
+  // k stride padded to a multiple of 4 nodes: rows then start on 16-byte
+  // boundaries in FP64 and FP32 arrays, as the TMA tensor maps of the
+  // staged sweeps require (the pad nodes are never read as data)
+  D.N2 = (D.E2 + 1 + 3) & ~3;
   D.Nn = (long long)(D.E0 + 1) * D.N1 * D.N2;
   if (D.Nn > 0xffffffffLL) {
     set_error("more than 2^32 nodes per face", "init");
     return -1;
   }
   GCS_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  if (prepare_flux_f64() != 0 || prepare_flux_f32() != 0) {
+    set_error("staged flux sweeps cannot be configured on this device", "init");
+    return -1;
+  }
 
   // ---- one pool for every node array
   const long long per = kFaces * D.Nn;
@@ -1027,6 +1037,41 @@ int Context::set_bulk_split(double b0_threshold) {
     }
   }
   return 0;
+}
+
+}  // namespace gcs
+
+namespace gcs {
+
+// Tensor map of one node array of all six faces, viewed as the 3-D tensor
+// (k: N2, j: N1, face * N0 + i: 6 N0) with k contiguous, for the TMA-staged
+// sweeps.  The driver's encoder is reached through the runtime's entry-point
+// query, so the library links the runtime only.
+int encode_cell_map(CUtensorMap *map, const void *base, int elem_bytes, const Dims &D,
+                    int box_x, int box_y, int box_z) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (encode == nullptr) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || fn == nullptr)
+      return -1;
+    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  if (((size_t)base & 15) != 0 || (elem_bytes != 4 && elem_bytes != 8)) return -1;
+  const cuuint64_t dims[3] = {(cuuint64_t)D.N2, (cuuint64_t)D.N1,
+                              (cuuint64_t)kFaces * (cuuint64_t)(D.E0 + 1)};
+  const cuuint64_t strides[2] = {(cuuint64_t)D.N2 * elem_bytes,
+                                 (cuuint64_t)D.N2 * D.N1 * elem_bytes};
+  const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_z};
+  const cuuint32_t estride[3] = {1, 1, 1};
+  const CUresult r = encode(
+      map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+      3, const_cast<void *>(base), dims, strides, box, estride,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -1;
 }
 
 }  // namespace gcs

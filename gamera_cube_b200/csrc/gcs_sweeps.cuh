@@ -26,6 +26,7 @@
 #include "gcs_kernel_util.cuh"
 #include "gcs_kernels.cuh"
 #include "gcs_physics.cuh"
+#include "gcs_flux_tma.cuh"
 
 namespace gcs {
 
@@ -550,6 +551,15 @@ struct Sweeps {
                    cudaStream_t s) {
     const Dims &D = X.D;
     int a, n;
+    if (X.flux_staged) {
+      if (clamp_range(D.g, D.g + D.nr + 1, i0, i1, &a, &n))
+        launch_flux_tma<0, T>(X, B, O, a, a + n, s);
+      if (clamp_range(D.g, D.g + D.nr, i0, i1, &a, &n))
+        launch_flux_tma<1, T>(X, B, O, a, a + n, s);
+      if (clamp_range(D.g, D.g + D.nr, i0, i1, &a, &n))
+        launch_flux_tma<2, T>(X, B, O, a, a + n, s);
+      return;
+    }
     const Tile t = X.tile[kTileFlux];
     if (clamp_range(D.g, D.g + D.nr + 1, i0, i1, &a, &n))
       k_flux<0, T><<<tile_grid(n, D.n, D.n, t), tile_block(t), 0, s>>>(

@@ -238,7 +238,8 @@ enum {
   GCS_STAGE_HOST = 16,
   GCS_STAGE_SOLVE_EDGE = 17,
   GCS_STAGE_OPTIONS = 18,
-  GCS_STAGE_PRESSURE_CONTROL = 19
+  GCS_STAGE_PRESSURE_CONTROL = 19,
+  GCS_STAGE_TILE_COPY = 20
 };
 
 /* Build a device context from a host grid in the reference layout
@@ -319,6 +320,10 @@ int gcs_context_reset_failure(gcs_context *ctx);
 uintptr_t gcs_context_stream(gcs_context *ctx);
 /* Profiling: record CUDA events around each stage of every step. */
 int gcs_context_set_profiling(gcs_context *ctx, int on);
+/* Flux sweeps with the Up7 stencil cells staged in shared memory by TMA
+ * (on = 1, the default) or read per face from global memory (on = 0); the
+ * two give the same fluxes bit for bit. */
+int gcs_context_set_flux_staging(gcs_context *ctx, int on);
 /* Accumulated device milliseconds and launch counts per stage since
  * profiling was switched on; returns the number of stages written. */
 int gcs_context_stage_times(gcs_context *ctx, double *ms, long long *calls,

@@ -38,9 +38,9 @@ from tests.parity_util import STATE_ARRAYS, compare_state, divergence
 pytestmark = pytest.mark.gpu
 
 RTOL_STEP = 1e-12
-# 100 chained steps: per-step differences of ~1e-15 (device libm, FMA in the
-# sweeps) accumulate; measured on B200 well below this bound.
-RTOL_CHAINED = 1e-9
+# 100 chained steps: the per-step differences (device libm, FMA in the
+# sweeps; ~6e-15) do not grow here: 8.9e-15 measured on B200 after 100 steps.
+RTOL_CHAINED = 1e-11
 C1 = (48, 32)             # radial, angular active cells per face
 C1_STEPS = 100
 
@@ -224,10 +224,12 @@ def _poison(case, what, face, cell):
         raise ValueError(what)
 
 
-# an active cell of face 2 at least seven cells from every seam and away
-# from the radial boundary layers, so no halo fill reads it
-_CASE = (12, 16)
-_CELL = (9, 12, 11)
+# an active cell of face 2 eleven cells or more from every seam, outside the
+# reference's 8 x 8 halo donor windows (whose zero-weight taps would carry a
+# NaN into the neighbour faces' ghosts, where the device's four-tap sum
+# does not), and away from the radial boundary layers
+_CASE = (12, 24)
+_CELL = (9, 16, 15)
 
 
 def _compare_with_nonfinite(gpu, ref):

@@ -8,10 +8,10 @@
 // copies (cp.async.bulk.tensor.3d) of the predicted primitives (5), the
 // predicted cell B (3) and the cell volume: the tile's cells plus the four
 // Up7 ghost cells on each side along the sweep axis (FY + 8 cells, or
-// FX + 8 for d = 2).  Two stages: the next tile's copies are in flight while
-// the current tile is computed from shared memory, so every cell value is
+// FX + 8 for d = 2).  The following tiles' copies are in flight while the
+// current tile is computed from shared memory, so every cell value is
 // read from HBM once per sweep instead of eight times, and no thread waits
-// on a global load of the stencil.  Per-face arrays (frame, area, interface
+// on a global load of the stencil.  (Three stages; see k_flux_tma.)  Per-face arrays (frame, area, interface
 // volume, normal field, B0) are read directly (coalesced along k).
 //
 // The last tile along the sweep axis also computes the extra face FY (FX for
@@ -19,9 +19,9 @@
 // their own.  The tensor maps are encoded on the host at every launch
 // (encode_cell_map, gcs_setup.cu) from the arrays of the Bulk view, so a
 // context that shares scratch arrays with another gets maps of the arrays it
-// reads.  Waits on the stage barriers are bounded: on expiry the block
-// records a kStageTileCopy failure, waits (bounded again) for its other
-// stage and returns.
+// reads.  Waits on the stage barriers are bounded: on expiry a warp
+// records a kStageTileCopy failure, waits (bounded again) for the other
+// stages' copies and returns.
 #pragma once
 
 #include <cuda.h>
@@ -44,9 +44,11 @@ struct FluxTile {
   static constexpr int VARS = 9;                    // 5 primitives, 3 B, volume
   static constexpr unsigned VAR_BYTES = (unsigned)(CELLS * sizeof(T));
   static constexpr unsigned STAGE_BYTES = VARS * VAR_BYTES;
-  // two stages, 128 bytes of alignment slack, the two stage barriers and
-  // the block's abort flag
-  static constexpr size_t SMEM = 2 * (size_t)STAGE_BYTES + 128 + 32;
+  static constexpr int STAGES = 3;
+  // the stage buffers, 128 bytes of alignment slack, the stage barriers,
+  // the per-stage counters and a flag
+  static constexpr size_t SMEM = STAGES * (size_t)STAGE_BYTES + 128 + 8 * STAGES +
+                                 4 * STAGES + 4;
   // smem distance between consecutive stencil cells
   static constexpr int STEP = d == 2 ? 1 : FX;
   static_assert(VAR_BYTES % 128 == 0, "TMA destinations need 128-byte alignment");
@@ -306,66 +308,93 @@ __device__ __forceinline__ void tile_face(const T *sm, const TileCoord &c, int x
   staged_face<d, T>(sm, s0, D, S, B, O, st, c.f, i, j, k);
 }
 
+// Warps of a staged flux block.  They share the stage buffers but never wait
+// for one another: a warp waits only for the copies of the stage it is about
+// to read, and the last warp to finish reading a stage issues its refill
+// (the tile kStages iterations ahead).  The extra faces of a last tile along
+// the sweep axis go to one warp, a different warp on each iteration.
 template <int d, typename T>
 __global__ void __launch_bounds__(256, 2)
     k_flux_tma(const __grid_constant__ FluxMaps maps, Dims D, DevState S, Bulk<T> B,
                Opts O, DevStatus *st, FluxTiles L) {
   using Sh = FluxTile<d, T>;
+  constexpr int kWarps = Sh::THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  // stage buffers on a 128-byte boundary (TMA destinations), then the
-  // barriers and the abort flag
+  // stage buffers on a 128-byte boundary (TMA destinations), then the stage
+  // barriers, the per-stage count of warps done with the stage, and a flag
   unsigned char *base =
       smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
-  T *stage[2] = {(T *)base, (T *)(base + Sh::STAGE_BYTES)};
-  unsigned long long *bar = (unsigned long long *)(base + 2 * Sh::STAGE_BYTES);
-  int &abort_flag = *(int *)(bar + 2);
-  const int tid = threadIdx.x;
+  unsigned long long *full = (unsigned long long *)(base + Sh::STAGES * Sh::STAGE_BYTES);
+  int *done = (int *)(full + Sh::STAGES);
+  int &skip = done[Sh::STAGES];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long first = blockIdx.x, stride = gridDim.x;
   // a block leaves before its first copy if an earlier kernel of the step
   // failed (one thread reads the status, so the whole block agrees)
-  if (tid == 0) abort_flag = failed(st) ? 1 : 0;
-  __syncthreads();
-  if (abort_flag) return;
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[0])));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[1])));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    issue_tile<d, T>(maps, D, L, first, stage[0], &bar[0]);
-    if (first + stride < L.count)
-      issue_tile<d, T>(maps, D, L, first + stride, stage[1], &bar[1]);
+    skip = failed(st) ? 1 : 0;
+    if (!skip) {
+      for (int q = 0; q < Sh::STAGES; ++q) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[q])));
+        done[q] = 0;
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      for (int q = 0; q < Sh::STAGES; ++q)
+        if (first + q * stride < L.count)
+          issue_tile<d, T>(maps, D, L, first + q * stride,
+                           (T *)(base + q * Sh::STAGE_BYTES), &full[q]);
+    }
   }
   __syncthreads();
+  if (skip) return;
   unsigned it = 0;
   for (long long t = first; t < L.count; t += stride, ++it) {
-    const int s = it & 1;
-    if (tid == 0 && !bar_wait(&bar[s], (it >> 1) & 1u, kTileSpinLimit)) abort_flag = 1;
-    __syncthreads();
-    if (abort_flag) {
-      // the copies of this stage did not arrive: record it, and wait (bounded)
-      // for the other stage's copies before the block's shared memory is
-      // released
-      if (tid == 0) {
+    const int s = (int)(it % Sh::STAGES);
+    const unsigned phase = (it / Sh::STAGES) & 1u;
+    unsigned ok = 1;
+    if (lane == 0) ok = bar_wait(&full[s], phase, kTileSpinLimit) ? 1u : 0u;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (!ok) {
+      // the copies of this stage did not arrive: record it, then wait
+      // (bounded) for the copies of the other stages before leaving, so no
+      // copy lands in shared memory the block has released
+      if (lane == 0) {
         fail(st, kStageTileCopy, d, 0, 0, 0, 0);
-        if (t + stride < L.count) bar_wait(&bar[s ^ 1], ((it + 1) >> 1) & 1u, kTileSpinLimit);
+        for (int q = 1; q < Sh::STAGES; ++q)
+          if (t + q * stride < L.count)
+            bar_wait(&full[(s + q) % Sh::STAGES], ((it + q) / Sh::STAGES) & 1u,
+                     kTileSpinLimit);
       }
       return;
     }
     const TileCoord c = tile_coord<d, T>(L, t);
-    const T *sm = stage[s];
+    const T *sm = (const T *)(base + s * Sh::STAGE_BYTES);
     {
       const int x = tid % Sh::FX, y = tid / Sh::FX;
       if (x < c.fb && y < c.fa) tile_face<d, T>(sm, c, x, y, L, D, S, B, O, st);
     }
-    // the extra face of a last tile along the sweep axis
-    if (d == 2) {
-      if (c.fb > Sh::FX && tid < c.fa) tile_face<d, T>(sm, c, Sh::FX, tid, L, D, S, B, O, st);
-    } else {
-      if (c.fa > Sh::FY && tid < c.fb) tile_face<d, T>(sm, c, tid, Sh::FY, L, D, S, B, O, st);
+    // the extra faces of a last tile along the sweep axis, by one warp
+    if (warp == (int)(it % kWarps)) {
+      if (d == 2) {
+        if (c.fb > Sh::FX && lane < c.fa) tile_face<d, T>(sm, c, Sh::FX, lane, L, D, S, B, O, st);
+      } else {
+        if (c.fa > Sh::FY && lane < c.fb) tile_face<d, T>(sm, c, lane, Sh::FY, L, D, S, B, O, st);
+      }
     }
-    __syncthreads();   // every thread is done with this stage
-    if (tid == 0 && t + 2 * stride < L.count)
-      issue_tile<d, T>(maps, D, L, t + 2 * stride, stage[s], &bar[s]);
+    // this warp is done with the stage; the last warp refills it
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      if (atomicAdd(&done[s], 1) == kWarps - 1) {
+        done[s] = 0;
+        const long long next = t + (long long)Sh::STAGES * stride;
+        if (next < L.count) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          issue_tile<d, T>(maps, D, L, next, (T *)(base + s * Sh::STAGE_BYTES), &full[s]);
+        }
+      }
+    }
   }
 }
 

@@ -45,6 +45,9 @@ struct FluxTile {
   static constexpr unsigned VAR_BYTES = (unsigned)(CELLS * sizeof(T));
   static constexpr unsigned STAGE_BYTES = VARS * VAR_BYTES;
   static constexpr int STAGES = 3;
+  // resident blocks per SM the kernel is compiled for: 2 (128 registers) in
+  // FP64, 4 (64 registers) in FP32
+  static constexpr int MIN_BLOCKS = sizeof(T) == 8 ? 2 : 4;
   // the stage buffers, 128 bytes of alignment slack, the stage barriers,
   // the per-stage counters and a flag
   static constexpr size_t SMEM = STAGES * (size_t)STAGE_BYTES + 128 + 8 * STAGES +
@@ -255,15 +258,9 @@ __device__ __forceinline__ void staged_face(const T *sm, int s0, const Dims &D,
     if (O.hogs)
       apply_hogs(&fl, &mx, (T)O.hogs_h, (T)O.hogs_m, O.s_boris, (T)O.s_c);
     if (O.hogs && O.s_boris) {
-      T lo[5], hi[5];
-#pragma unroll
-      for (int m = 0; m < 5; ++m) {
-        lo[m] = (T)S.Up[m][c - sd];
-        hi[m] = (T)S.Up[m][c];
-      }
       bool applied;
       T speed;
-      if (emergency_diffusion(&fl, st2, lo, hi, (T)O.s_c, &applied, &speed)) {
+      if (emergency_diffusion(&fl, st2, S.Up, c - sd, c, (T)O.s_c, &applied, &speed)) {
         fail(st, kStageEmergency, d, f, i, j, k);
         return;
       }
@@ -314,7 +311,7 @@ __device__ __forceinline__ void tile_face(const T *sm, const TileCoord &c, int x
 // (the tile kStages iterations ahead).  The extra faces of a last tile along
 // the sweep axis go to one warp, a different warp on each iteration.
 template <int d, typename T>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, FluxTile<d, T>::MIN_BLOCKS)
     k_flux_tma(const __grid_constant__ FluxMaps maps, Dims D, DevState S, Bulk<T> B,
                Opts O, DevStatus *st, FluxTiles L) {
   using Sh = FluxTile<d, T>;
@@ -352,9 +349,7 @@ __global__ void __launch_bounds__(256, 2)
   for (long long t = first; t < L.count; t += stride, ++it) {
     const int s = (int)(it % Sh::STAGES);
     const unsigned phase = (it / Sh::STAGES) & 1u;
-    unsigned ok = 1;
-    if (lane == 0) ok = bar_wait(&full[s], phase, kTileSpinLimit) ? 1u : 0u;
-    ok = __shfl_sync(0xffffffffu, ok, 0);
+    const bool ok = __all_sync(0xffffffffu, bar_wait(&full[s], phase, kTileSpinLimit));
     if (!ok) {
       // the copies of this stage did not arrive: record it, then wait
       // (bounded) for the copies of the other stages before leaving, so no
@@ -370,17 +365,27 @@ __global__ void __launch_bounds__(256, 2)
     }
     const TileCoord c = tile_coord<d, T>(L, t);
     const T *sm = (const T *)(base + s * Sh::STAGE_BYTES);
-    {
-      const int x = tid % Sh::FX, y = tid / Sh::FX;
-      if (x < c.fb && y < c.fa) tile_face<d, T>(sm, c, x, y, L, D, S, B, O, st);
-    }
-    // the extra faces of a last tile along the sweep axis, by one warp
-    if (warp == (int)(it % kWarps)) {
-      if (d == 2) {
-        if (c.fb > Sh::FX && lane < c.fa) tile_face<d, T>(sm, c, Sh::FX, lane, L, D, S, B, O, st);
+    // the thread's face, then (one warp per iteration) the extra face of a
+    // last tile along the sweep axis; one call site keeps the face code
+    // once in the instruction stream
+    const int passes = warp == (int)(it % kWarps) ? 2 : 1;
+    for (int pass = 0; pass < passes; ++pass) {
+      int x, y;
+      bool on;
+      if (pass == 0) {
+        x = tid % Sh::FX;
+        y = tid / Sh::FX;
+        on = x < c.fb && y < c.fa;
+      } else if (d == 2) {
+        x = Sh::FX;
+        y = lane;
+        on = c.fb > Sh::FX && lane < c.fa;
       } else {
-        if (c.fa > Sh::FY && lane < c.fb) tile_face<d, T>(sm, c, lane, Sh::FY, L, D, S, B, O, st);
+        x = lane;
+        y = Sh::FY;
+        on = c.fa > Sh::FY && lane < c.fb;
       }
+      if (on) tile_face<d, T>(sm, c, x, y, L, D, S, B, O, st);
     }
     // this warp is done with the stage; the last warp refills it
     __syncwarp();

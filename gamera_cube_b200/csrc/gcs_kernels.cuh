@@ -39,7 +39,7 @@ struct Ctx {
   int n_edge_groups = 0;
   StepParams *params = nullptr;   // device
   DevStatus *status = nullptr;    // device
-  int flux_staged = 1;            // 1: TMA-staged flux sweeps (gcs_flux_tma.cuh)
+  int flux_staged = 0;            // 1: TMA-staged flux sweeps (gcs_flux_tma.cuh)
   int bulk = 0;                   // 1: FP32-bulk sweeps (B32)
   int bulk_split = 0;             // radial layers [0, bulk_split) stay FP64
   Bulk<float> B32{};

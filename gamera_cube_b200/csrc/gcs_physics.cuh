@@ -350,11 +350,14 @@ __device__ inline void apply_hogs(FluidFlux<T> *fl, MaxwellFlux<T> *mx, T ch, T 
   }
 }
 
-// nonorthogonal_flux.c:206-241 (use_boris is true at every call site)
+// nonorthogonal_flux.c:206-241 (use_boris is true at every call site).  The
+// conserved states either side of the face (U[m][lo], U[m][hi]) are read
+// only where the diffusion applies.
 template <typename T>
 __device__ inline int emergency_diffusion(FluidFlux<T> *fl, const PrimT<T> st[2],
-                                          const T lo[5], const T hi[5], T c,
-                                          bool *applied, T *speed) {
+                                          const double *const U[5], long long lo_at,
+                                          long long hi_at, T c, bool *applied,
+                                          T *speed) {
   *applied = false;
   T s2 = T(0.0);
 #pragma unroll
@@ -366,6 +369,12 @@ __device__ inline int emergency_diffusion(FluidFlux<T> *fl, const PrimT<T> st[2]
   const T is = Num<T>::sqrt_(T(0.5) * s2);
   *speed = is;
   if (is < T(1.5) * c) return 0;
+  T lo[5], hi[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    lo[m] = (T)U[m][lo_at];
+    hi[m] = (T)U[m][hi_at];
+  }
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
     if (!isfinite(lo[m]) || !isfinite(hi[m])) return 1;

@@ -219,15 +219,9 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, D
     if (O.hogs)
       apply_hogs(&fl, &mx, (T)O.hogs_h, (T)O.hogs_m, O.s_boris, (T)O.s_c);
     if (O.hogs && O.s_boris) {
-      T lo[5], hi[5];
-#pragma unroll
-      for (int m = 0; m < 5; ++m) {
-        lo[m] = (T)S.Up[m][c - sd];
-        hi[m] = (T)S.Up[m][c];
-      }
       bool applied;
       T speed;
-      if (emergency_diffusion(&fl, st2, lo, hi, (T)O.s_c, &applied, &speed)) {
+      if (emergency_diffusion(&fl, st2, S.Up, c - sd, c, (T)O.s_c, &applied, &speed)) {
         fail(st, kStageEmergency, d, f, i, j, k);
         return;
       }

@@ -321,8 +321,8 @@ uintptr_t gcs_context_stream(gcs_context *ctx);
 /* Profiling: record CUDA events around each stage of every step. */
 int gcs_context_set_profiling(gcs_context *ctx, int on);
 /* Flux sweeps with the Up7 stencil cells staged in shared memory by TMA
- * (on = 1, the default) or read per face from global memory (on = 0); the
- * two give the same fluxes bit for bit. */
+ * (on = 1) or read per face from global memory (on = 0, the default, the
+ * faster of the two on B200); the two give the same fluxes bit for bit. */
 int gcs_context_set_flux_staging(gcs_context *ctx, int on);
 /* Accumulated device milliseconds and launch counts per stage since
  * profiling was switched on; returns the number of stages written. */

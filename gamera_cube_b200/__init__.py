@@ -153,6 +153,8 @@ def _load(path=None):
     sig["gamera_cs_sync_edge_emf_planned"] = (C.c_int, [C.c_void_p, P(abi.Storage)])
     sig.update(abi.mi_dipole_signatures())
     sig.update(abi.ensemble_signatures())
+    sig["gcs_context_set_mi_coupling"] = (C.c_int, [C.c_void_p, C.c_void_p, C.c_int])
+    sig["gcs_context_time"] = (C.c_int, [C.c_void_p, P(C.c_double)])
     sig["gcs_context_mi_dipole_create"] = (
         C.c_int, [C.c_void_p, P(abi.EarthStartup), P(abi.MiDipoleConfig),
                   P(C.c_void_p)])

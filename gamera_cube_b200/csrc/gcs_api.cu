@@ -46,7 +46,7 @@ const char *kStageNames[] = {
     "edge_velocity",  "transverse_field", "edge_density",   "compute_edge_emf",
     "boris_after_hydro", "recover_B",    "recover_B",       "timestep",
     "host_callback",  "solve_edge_field", "options",        "pressure_control",
-    "tile_copy"};
+    "tile_copy",      "mi_coupling"};
 
 // Option checks of the reference step and of each stage it calls
 // (cubedsphere_step.c:23-47, nonorthogonal_sweep.c:48-62, 209-221,
@@ -156,12 +156,12 @@ bool set_timestep_opts(const gamera_no_timestep_options *t, gcs::Opts *O) {
 enum Slot {
   kSlotSeamPhi = 0, kSlotHalo, kSlotPredict, kSlotFlux, kSlotSeamFlux,
   kSlotEmf, kSlotEdgeSync, kSlotUpdate, kSlotSeamPhiFinal, kSlotRecover,
-  kSlotDt, kSlotCount
+  kSlotDt, kSlotMi, kSlotCount
 };
 const char *kSlotNames[kSlotCount] = {
     "seam_sync_phi", "halo", "predict", "flux", "seam_sync_flux",
     "edge_emf", "edge_sync", "ct_update", "seam_sync_phi_final",
-    "recover_cfl", "next_dt"};
+    "recover_cfl", "next_dt", "mi_coupling"};
 
 struct Marker {
   gcs_context *ctx;
@@ -235,6 +235,12 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
   const bool post_control = driver_mode && C.pc_on;
   Marker mk{ctx};
   mk.begin();
+  if (driver_mode && C.mi_graph != nullptr) {
+    // the ionosphere coupling on its device-side cadence, before the step
+    // (test_cubedsphere_dipole_background.c:631)
+    if (gcs::mi_launch_in_step(C.mi_graph, s) != 0) return -1;
+    mk.mark(kSlotMi);
+  }
   gcs::launch_seam_sync(X, 1, s);
   mk.mark(kSlotSeamPhi);
   gcs::launch_halo(X, s);
@@ -1044,6 +1050,7 @@ int context_run(gcs_context *ctx, const gamera_no_advance_options *options,
     return -1;
   O.dt_fraction = fraction;
   gcs::Context &C = ctx->c;
+  if (C.mi_graph != nullptr && gcs::mi_before_run(C.mi_graph) != 0) return -1;
   gcs::StepParams p;
   if (cudaMemcpyAsync(&p, C.X.params, sizeof(p), cudaMemcpyDeviceToHost,
                       C.stream) != cudaSuccess ||
@@ -1067,6 +1074,7 @@ int context_run(gcs_context *ctx, const gamera_no_advance_options *options,
     for (size_t q = 0; q < sizeof(O); ++q) key = (key ^ b[q]) * 1099511628211ULL;
     key = (key ^ (unsigned long long)C.X.bulk) * 1099511628211ULL;
     key = (key ^ (unsigned long long)(0x5354ULL + C.X.flux_staged)) * 1099511628211ULL;
+    key = (key ^ (unsigned long long)(uintptr_t)C.mi_graph) * 1099511628211ULL;
     if (es) {
       const unsigned char *e = (const unsigned char *)es->dev;
       for (size_t q = 0; q < sizeof(*es->dev); ++q) key = (key ^ e[q]) * 1099511628211ULL;
@@ -1095,11 +1103,18 @@ int context_run(gcs_context *ctx, const gamera_no_advance_options *options,
       C.graph_key = key;
     }
     for (int q = 0; q < steps; ++q)
-      if (cudaGraphLaunch(C.graph_exec, C.stream) != cudaSuccess) return -1;
+      if (cudaGraphLaunch(C.graph_exec, C.stream) != cudaSuccess) {
+        if (C.mi_graph != nullptr) gcs::mi_after_run(C.mi_graph);
+        return -1;
+      }
   } else {
     for (int q = 0; q < steps; ++q)
-      if (run_step(ctx, O, 1, nullptr, es) != 0) return -1;
+      if (run_step(ctx, O, 1, nullptr, es) != 0) {
+        if (C.mi_graph != nullptr) gcs::mi_after_run(C.mi_graph);
+        return -1;
+      }
   }
+  if (C.mi_graph != nullptr) gcs::mi_after_run(C.mi_graph);
   return 0;
 }
 
@@ -1133,6 +1148,17 @@ int gcs_context_sync(gcs_context *ctx) {
     report_failure(ctx->c);
     return -1;
   }
+  return 0;
+}
+
+int gcs_context_time(gcs_context *ctx, double *time) {
+  if (!ctx || !time) return -1;
+  gcs::StepParams p;
+  if (cudaMemcpyAsync(&p, ctx->c.X.params, sizeof(p), cudaMemcpyDeviceToHost,
+                      ctx->c.stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->c.stream) != cudaSuccess)
+    return -1;
+  *time = p.time;
   return 0;
 }
 

@@ -11,6 +11,8 @@
 #include "gcs_kernels.cuh"
 #include "gcs_topology.h"
 
+struct gamera_cs_mi_dipole;
+
 namespace gcs {
 
 enum ArrayKind {
@@ -65,6 +67,9 @@ struct Context {
   int pc_on = 0;
   double *pc_dipole = nullptr;
   void *pc_stats = nullptr;
+  // ionosphere coupling updated inside the driver loop's step graph
+  // (gcs_context_set_mi_coupling), or null
+  ::gamera_cs_mi_dipole *mi_graph = nullptr;
   // per-stage timing (profiling mode)
   int profiling = 0;
   double stage_ms[16] = {0};
@@ -120,6 +125,12 @@ struct Context {
     return true;
   }
 };
+
+// gcs_mi_dipole.cu: the coupling update inside the driver loop's step
+int mi_launch_in_step(::gamera_cs_mi_dipole *s, cudaStream_t st);
+int mi_before_run(::gamera_cs_mi_dipole *s);
+void mi_after_run(::gamera_cs_mi_dipole *s);
+const double *mi_graph_potential(const ::gamera_cs_mi_dipole *s, const Context *C);
 
 // gcs_pressure.cu
 int pressure_prepare(Context &C, const gamera_no_grid *grid);

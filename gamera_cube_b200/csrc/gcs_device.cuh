@@ -161,6 +161,7 @@ enum Stage : int {
   kStageOptions = 18,
   kStagePressureControl = 19,
   kStageTileCopy = 20,   // a staged sweep's tile copy did not arrive in time
+  kStageMiCoupling = 21, // an ionosphere coupling update inside the step failed
 };
 
 struct DevStatus {

@@ -840,6 +840,13 @@ int earth_sync_mi(gcs_earth *e, const gamera_cs_mi_dipole *mi) {
   EarthDev &E = e->dev;
   MiLookup L;
   double norm;
+  if (mi != nullptr && mi_lookup_device(mi, e->C, &L, &norm)) {
+    // updated inside the step graph: the wall reads the device potential
+    E.mil = L;
+    E.mi_potential_norm = norm;
+    E.mi = 1;
+    return 0;
+  }
   if (mi == nullptr || !mi_lookup(mi, &L, &norm)) {
     E.mi = 0;
     return 0;

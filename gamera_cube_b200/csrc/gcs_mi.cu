@@ -68,6 +68,7 @@ struct System {
   int np, nt;
   int max_iter;
   int pad;
+  const int *gate;  // when set, the solve runs only where *gate != 0
   double pe;        // pole edge coefficient (nonorthogonal_mi.c:324-334)
   double neg_r2;    // -R^2
   double low;       // low-latitude Dirichlet potential
@@ -190,6 +191,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   const System S = systems[blockIdx.x / csize];
+  // a gated solve that is not due: every CTA of the cluster leaves here,
+  // before any cluster barrier
+  if (S.gate != nullptr && *S.gate == 0) return;
   const int np = S.np, R = S.nt - 2;
   const int t = threadIdx.x;
 
@@ -423,6 +427,7 @@ __global__ void __launch_bounds__(col_threads(MR), 1)
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   const System &S = systems[blockIdx.x / csize];
+  if (S.gate != nullptr && *S.gate == 0) return;
   const int np = S.np, R = S.nt - 2;
   const int j = threadIdx.x;
   const bool on = j < np;
@@ -1070,6 +1075,7 @@ gcs_mi_plan *plan_create(const gamera_mi_solver_config *configs, int count) {
     S.nt = p->nt;
     S.max_iter = c->maximum_iterations;
     S.pad = 0;
+    S.gate = nullptr;
     S.pe = pole_edge(c);
     S.neg_r2 = -(c->ionosphere_radius_m * c->ionosphere_radius_m);
     S.low = c->low_latitude_potential_v;
@@ -1122,6 +1128,37 @@ int plan_launch(gcs_mi_plan *p, cudaStream_t stream) {
 
 std::mutex g_cache_mutex;
 gcs_mi_plan *g_cache = nullptr;  // plan of the last drop-in call
+
+}  // namespace
+
+namespace gcs {
+
+// A plan whose solves run only where *gate != 0 (a coupling update gated by
+// its device-side cadence), bound to fixed FAC and potential arrays.  Both
+// are set outside any stream capture; the plan's later launches on the same
+// arrays need no host synchronisation.
+int mi_plan_gate(gcs_mi_plan *p, const int *gate, const double *fac, double *pot) {
+  if (!p) return -1;
+  for (int q = 0; q < p->count; ++q) p->host_sys[q].gate = gate;
+  for (int q = 0; q < p->count; ++q) {
+    p->host_sys[q].fac = fac + q * (size_t)p->np * p->nt;
+    p->host_sys[q].pot = pot + q * (size_t)p->np * p->nt;
+  }
+  return cuda_ok(cudaMemcpy(p->d_sys, p->host_sys.data(), p->count * sizeof(System),
+                            cudaMemcpyHostToDevice),
+                 "cudaMemcpy")
+             ? 0
+             : -1;
+}
+
+// Device status words of a plan's solves (0 converged, 1 not converged,
+// 2 non-finite FAC) and its launch.
+const int *mi_plan_status(const gcs_mi_plan *p) { return p ? p->d_status : nullptr; }
+int mi_plan_launch(gcs_mi_plan *p, cudaStream_t stream) { return plan_launch(p, stream); }
+
+}  // namespace gcs
+
+namespace {
 
 gcs_mi_plan *cached_plan(const gamera_mi_solver_config *config) {
   if (g_cache && g_cache->count == 1 &&

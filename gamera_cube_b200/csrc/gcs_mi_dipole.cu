@@ -20,6 +20,15 @@
 // potential and FAC are then copied to the host, where the reference-layout
 // entry points (potential lookup, wall EMF, ghost E x B drift, statistics,
 // CSV and analysis views) read them.
+//
+// Cadence on the device.  Attached to its context's driver loop
+// (gcs_context_set_mi_coupling), the update runs inside the step's CUDA
+// graph: k_mi_due evaluates the reference's rule (cubedsphere_mi_dipole.c:
+// 372-378, 430-435) from the step parameters' simulation time, or every
+// n-th step, and sets a gate that every kernel of the update, the cluster
+// solve included, reads first; k_mi_check turns a non-finite FAC or an
+// unconverged solve into a step failure.  The host copies of potential,
+// FAC, statistics and cadence are then refreshed on the next host access.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -33,12 +42,31 @@
 #include "gcs_error.h"
 #include "gcs_topology.h"
 #include "gcs_mi_lookup.cuh"
+#include "gcs_kernel_util.cuh"
 
 using gcs::set_api_error;
+
+namespace gcs {
+// gcs_mi.cu: gated, array-bound solve plans
+int mi_plan_gate(gcs_mi_plan *p, const int *gate, const double *fac, double *pot);
+const int *mi_plan_status(const gcs_mi_plan *p);
+int mi_plan_launch(gcs_mi_plan *p, cudaStream_t stream);
+}  // namespace gcs
 
 namespace {
 
 constexpr int kHemispheres = 2;
+
+// Device-side cadence of one coupling (the host's ready / epoch /
+// next-update state, mirrored) and the gate of the current update.
+struct MiCadence {
+  double next_update_s, epoch_s;
+  double length_norm_m, speed_norm_m_s;   // code time -> seconds, as the host
+  double interval_s;     // coupling interval
+  int ready, due;        // due: the gate every kernel of an update reads
+  int every;             // > 0: every n-th step; 0: the reference's time rule
+  int pad;
+};
 
 struct FringeB {      // one fringe cell of the shell field
   double wx, wy;
@@ -99,7 +127,8 @@ struct FieldPtrs {
   const double *b[3];            // residual cell B per component
 };
 
-__global__ void k_shell_field(FieldPtrs B, MiDev M) {
+__global__ void k_shell_field(FieldPtrs B, MiDev M, const int *gate) {
+  if (*gate == 0) return;
   const long long per = 3LL * M.S * M.S;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 6 * per) return;
@@ -160,7 +189,8 @@ __device__ double edge_integral(const MiDev &M, int f, int dir, int i, int j, in
   return d * e.len;
 }
 
-__global__ void k_shell_current(gcs::DevGeom G, MiDev M) {
+__global__ void k_shell_current(gcs::DevGeom G, MiDev M, const int *gate) {
+  if (*gate == 0) return;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long per = (long long)M.n * M.n;
   if (t >= 6 * per) return;
@@ -202,7 +232,8 @@ __global__ void k_shell_current(gcs::DevGeom G, MiDev M) {
   M.shell_fac[(size_t)f * M.S * M.S + (size_t)(jj + 1) * M.S + kk + 1] = fac;
 }
 
-__global__ void k_shell_fringe(MiDev M) {
+__global__ void k_shell_fringe(MiDev M, const int *gate) {
+  if (*gate == 0) return;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long per = (long long)M.S * M.S;
   if (t >= 6 * per) return;
@@ -217,7 +248,8 @@ __global__ void k_shell_fringe(MiDev M) {
   M.shell_fac[t] = fac;
 }
 
-__global__ void k_polar_sample(MiDev M) {
+__global__ void k_polar_sample(MiDev M, const int *gate) {
+  if (*gate == 0) return;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)kHemispheres * M.polar_count) return;
   const Sample &P = M.samples[t];
@@ -232,6 +264,49 @@ __global__ void k_polar_sample(MiDev M) {
   const double v = (1.0 - P.wx) * lower + P.wx * upper;
   if (!isfinite(v)) atomicExch(M.status, 1);
   M.fac[t] = v;
+}
+
+// An update requested by the host: open the gate, clear the FAC status.
+__global__ void k_open_gate(MiCadence *c, int *status) {
+  c->due = 1;
+  *status = 0;
+}
+
+// The cadence of an update inside the step graph, before the step:
+// the reference's rule on the simulation time of the state (seconds
+// = code time x time_scale), or every n-th step.  A due update advances the
+// cadence as the host does after an update (the step fails if the update
+// does, so the advance is never seen without it).
+__global__ void k_mi_due(const gcs::StepParams *prm, MiCadence *c, int *status,
+                         const gcs::DevStatus *st) {
+  if (gcs::failed(st)) {
+    c->due = 0;
+    return;
+  }
+  const double time_s = prm->time * c->length_norm_m / c->speed_norm_m_s;
+  int due;
+  if (c->every > 0)
+    due = !c->ready || prm->step % c->every == 0;
+  else
+    due = !c->ready || time_s + 1e-10 >= c->next_update_s;
+  c->due = due;
+  if (!due) return;
+  *status = 0;
+  c->ready = 1;
+  c->epoch_s = time_s;
+  if (c->every == 0) {
+    do {
+      c->next_update_s += c->interval_s;
+    } while (c->next_update_s <= time_s + 1e-10);
+  }
+}
+
+// A failed update inside the step graph fails the step.
+__global__ void k_mi_check(const MiCadence *c, const int *fac_status,
+                           const int *solve_status, gcs::DevStatus *st) {
+  if (c->due == 0) return;
+  if (*fac_status != 0 || solve_status[0] != 0 || solve_status[1] != 0)
+    gcs::fail(st, gcs::kStageMiCoupling, 0, 0, 0, 0, 0);
 }
 
 double vdot(const gamera_no_vec3 &a, const gamera_no_vec3 &b) {
@@ -333,6 +408,11 @@ struct gamera_cs_mi_dipole {
   MiDev dev{};
   gcs_mi_plan *solver = nullptr;
   double *d_pot = nullptr;  // 2 x nt x np (warm start)
+  MiCadence *d_cad = nullptr;  // device cadence and update gate
+  int every = 0;               // cadence of the in-graph update (0: time rule)
+  int in_graph = 0;            // attached to its context's driver loop
+  int stale = 0;               // host copies older than the device's
+  int push = 0;                // host cadence newer than the device's
   // host copies of the last solved state
   std::vector<double> fac[kHemispheres], pot[kHemispheres];
   std::vector<double> host_shell_fac;  // 6 x S^2
@@ -357,8 +437,58 @@ gcs::MiLookup lookup_of(const gamera_cs_mi_dipole *s) {
   return L;
 }
 
+bool cuda_ok(cudaError_t e, const char *what);
+
+// Host copies (cadence, potential, FAC, statistics) from the device after
+// updates that ran inside the step graph.
+int sync_host(const gamera_cs_mi_dipole *cs) {
+  gamera_cs_mi_dipole *s = const_cast<gamera_cs_mi_dipole *>(cs);
+  if (s == nullptr || !s->stale || s->ctx == nullptr) return 0;
+  s->stale = 0;
+  MiCadence c;
+  if (!cuda_ok(cudaStreamSynchronize(s->ctx->stream), "MI coupling") ||
+      !cuda_ok(cudaMemcpy(&c, s->d_cad, sizeof(c), cudaMemcpyDeviceToHost), "cudaMemcpy"))
+    return -1;
+  s->ready = c.ready;
+  s->epoch_s = c.epoch_s;
+  s->next_update_s = c.next_update_s;
+  if (!c.ready) return 0;
+  const size_t count = (size_t)s->np * s->nt;
+  for (int h = 0; h < kHemispheres; ++h)
+    if (!cuda_ok(cudaMemcpy(s->pot[h].data(), s->d_pot + h * count, count * sizeof(double),
+                            cudaMemcpyDeviceToHost), "cudaMemcpy") ||
+        !cuda_ok(cudaMemcpy(s->fac[h].data(), s->dev.fac + h * count,
+                            count * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy"))
+      return -1;
+  if (!cuda_ok(cudaMemcpy(s->host_shell_fac.data(), s->dev.shell_fac,
+                          s->host_shell_fac.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost), "cudaMemcpy"))
+    return -1;
+  return gcs_mi_plan_results(s->solver, s->solve, nullptr);
+}
+
+// The device cadence from the host's, before a step graph runs.
+int push_cadence(gamera_cs_mi_dipole *s) {
+  if (!s->push || s->d_cad == nullptr) return 0;
+  MiCadence c{};
+  c.next_update_s = s->next_update_s;
+  c.epoch_s = s->epoch_s;
+  c.length_norm_m = s->config.length_norm_m;
+  c.speed_norm_m_s = s->config.speed_norm_m_s;
+  c.interval_s = s->config.coupling_interval_s;
+  c.ready = s->ready;
+  c.due = 0;
+  c.every = s->every;
+  if (!cuda_ok(cudaStreamSynchronize(s->ctx->stream), "MI coupling") ||
+      !cuda_ok(cudaMemcpy(s->d_cad, &c, sizeof(c), cudaMemcpyHostToDevice), "cudaMemcpy"))
+    return -1;
+  s->push = 0;
+  return 0;
+}
+
 void destroy_state(gamera_cs_mi_dipole *s) {
   if (!s) return;
+  if (s->ctx != nullptr && s->ctx->mi_graph == s) s->ctx->mi_graph = nullptr;
   if (s->solver) gcs_mi_plan_destroy(s->solver);
   cudaFree(s->pool);
   delete s;
@@ -576,6 +706,7 @@ int build_coupling(gamera_cs_mi_dipole *s, gcs::Context &C, const GeomView &G,
   const size_t o_fac = take(npolar * sizeof(double));
   const size_t o_pot = take(npolar * sizeof(double));
   const size_t o_status = take(sizeof(int));
+  const size_t o_cad = take(sizeof(MiCadence));
   if (!cuda_ok(cudaMalloc(&s->pool, off), "cudaMalloc")) return -1;
   char *base = (char *)s->pool;
   if (!cuda_ok(cudaMemset(s->pool, 0, off), "cudaMemset") ||
@@ -615,6 +746,7 @@ int build_coupling(gamera_cs_mi_dipole *s, gcs::Context &C, const GeomView &G,
   M.polar_count = nt * np;
   M.status = (int *)(base + o_status);
   s->d_pot = (double *)(base + o_pot);
+  s->d_cad = (MiCadence *)(base + o_cad);
   // the two hemisphere solves (cubedsphere_mi_dipole.c:414-424)
   gamera_mi_solver_config sc[kHemispheres];
   for (int h = 0; h < kHemispheres; ++h) {
@@ -632,7 +764,11 @@ int build_coupling(gamera_cs_mi_dipole *s, gcs::Context &C, const GeomView &G,
     c.absolute_tolerance = 0.0;
   }
   if (gcs_mi_plan_create(sc, kHemispheres, &s->solver) != 0) return -1;
+  // every solve of this coupling is gated by its cadence and bound to its
+  // FAC and potential arrays
+  if (gcs::mi_plan_gate(s->solver, &s->d_cad->due, M.fac, s->d_pot) != 0) return -1;
   s->host_shell_fac.assign(nfac, 0.0);
+  s->push = 1;
   return 0;
 }
 
@@ -653,14 +789,13 @@ int run_update(gamera_cs_mi_dipole *s) {
   const long long nf = 6LL * 3 * M.S * M.S, nc = 6LL * M.n * M.n, ns = 6LL * M.S * M.S;
   const long long np = (long long)kHemispheres * M.polar_count;
   const FieldPtrs bp{{C.X.S.B[0], C.X.S.B[1], C.X.S.B[2]}};
-  bool ok = cuda_ok(cudaMemsetAsync(M.status, 0, sizeof(int), st), "cudaMemsetAsync");
-  if (ok) {
-    k_shell_field<<<(unsigned)((nf + bs - 1) / bs), bs, 0, st>>>(bp, M);
-    k_shell_current<<<(unsigned)((nc + bs - 1) / bs), bs, 0, st>>>(C.X.G, M);
-    k_shell_fringe<<<(unsigned)((ns + bs - 1) / bs), bs, 0, st>>>(M);
-    k_polar_sample<<<(unsigned)((np + bs - 1) / bs), bs, 0, st>>>(M);
-    ok = cuda_ok(cudaGetLastError(), "MI coupling launch");
-  }
+  const int *gate = &s->d_cad->due;
+  k_open_gate<<<1, 1, 0, st>>>(s->d_cad, M.status);
+  k_shell_field<<<(unsigned)((nf + bs - 1) / bs), bs, 0, st>>>(bp, M, gate);
+  k_shell_current<<<(unsigned)((nc + bs - 1) / bs), bs, 0, st>>>(C.X.G, M, gate);
+  k_shell_fringe<<<(unsigned)((ns + bs - 1) / bs), bs, 0, st>>>(M, gate);
+  k_polar_sample<<<(unsigned)((np + bs - 1) / bs), bs, 0, st>>>(M, gate);
+  bool ok = cuda_ok(cudaGetLastError(), "MI coupling launch");
   int status = 0;
   ok = ok && cuda_ok(cudaMemcpyAsync(&status, M.status, sizeof(int),
                                      cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync") &&
@@ -811,7 +946,7 @@ int gamera_cs_mi_dipole_create_potential_view(const gamera_cs_earth_startup *sta
 
 namespace gcs {
 bool mi_lookup(const gamera_cs_mi_dipole *s, MiLookup *L, double *potential_norm_v) {
-  if (s == nullptr || !s->ready) return false;
+  if (s == nullptr || sync_host(s) != 0 || !s->ready) return false;
   *L = lookup_of(s);
   *potential_norm_v = s->potential_norm_v;
   return true;
@@ -821,12 +956,14 @@ bool mi_lookup(const gamera_cs_mi_dipole *s, MiLookup *L, double *potential_norm
 extern "C" {
 
 int gamera_cs_mi_dipole_ready(const gamera_cs_mi_dipole *s) {
+  if (s != nullptr && sync_host(s) != 0) return 0;
   return s != nullptr && s->ready;
 }
 
 // cubedsphere_mi_dipole.c:372-378
 int gamera_cs_mi_dipole_update_due(const gamera_cs_mi_dipole *s, double time_code) {
   if (s == nullptr || !std::isfinite(time_code) || time_code < 0.0) return -1;
+  if (sync_host(s) != 0) return -1;
   const double time_s = time_code * s->config.length_norm_m / s->config.speed_norm_m_s;
   return !s->ready || time_s + 1e-10 >= s->next_update_s;
 }
@@ -843,6 +980,7 @@ int gamera_cs_mi_dipole_maybe_update(gamera_cs_mi_dipole *s, double time_code) {
   do {
     s->next_update_s += s->config.coupling_interval_s;
   } while (s->next_update_s <= time_s + 1e-10);
+  s->push = 1;
   return 1;
 }
 
@@ -865,7 +1003,8 @@ int gamera_cs_mi_dipole_import_potential(gamera_cs_mi_dipole *s, const double *v
                                          size_t count, double epoch_s,
                                          double next_update_s) {
   if (s == nullptr || values == nullptr || !std::isfinite(epoch_s) ||
-      !std::isfinite(next_update_s) || epoch_s < 0.0 || next_update_s <= epoch_s)
+      !std::isfinite(next_update_s) || epoch_s < 0.0 || next_update_s <= epoch_s ||
+      sync_host(s) != 0)
     return -1;
   const size_t per = (size_t)s->np * s->nt;
   if (count != kHemispheres * per) return -1;
@@ -880,6 +1019,7 @@ int gamera_cs_mi_dipole_import_potential(gamera_cs_mi_dipole *s, const double *v
   s->epoch_s = epoch_s;
   s->next_update_s = next_update_s;
   s->ready = 1;
+  s->push = 1;
   return 0;
 }
 
@@ -1037,6 +1177,89 @@ int gamera_cs_mi_dipole_write_shell_current_csv(const gamera_cs_mi_dipole *s,
                 asin(p.value[2] / r) * 180.0 / pi, phi, shell_jparallel(s, f, (int)j, (int)k));
       }
   return fclose(file) == 0 ? 0 : -1;
+}
+
+}  // extern "C"
+
+namespace gcs {
+
+// The coupling update inside a step of the device driver loop, before the
+// step: cadence, gated FAC kernels and solve, failure check.
+int mi_launch_in_step(gamera_cs_mi_dipole *s, cudaStream_t st) {
+  Context &C = *s->ctx;
+  MiDev &M = s->dev;
+  const int bs = 128;
+  const long long nf = 6LL * 3 * M.S * M.S, nc = 6LL * M.n * M.n, ns = 6LL * M.S * M.S;
+  const long long np = (long long)kHemispheres * M.polar_count;
+  const FieldPtrs bp{{C.X.S.B[0], C.X.S.B[1], C.X.S.B[2]}};
+  const int *gate = &s->d_cad->due;
+  k_mi_due<<<1, 1, 0, st>>>(C.X.params, s->d_cad, M.status, C.X.status);
+  k_shell_field<<<(unsigned)((nf + bs - 1) / bs), bs, 0, st>>>(bp, M, gate);
+  k_shell_current<<<(unsigned)((nc + bs - 1) / bs), bs, 0, st>>>(C.X.G, M, gate);
+  k_shell_fringe<<<(unsigned)((ns + bs - 1) / bs), bs, 0, st>>>(M, gate);
+  k_polar_sample<<<(unsigned)((np + bs - 1) / bs), bs, 0, st>>>(M, gate);
+  if (mi_plan_launch(s->solver, st) != 0) return -1;
+  k_mi_check<<<1, 1, 0, st>>>(s->d_cad, M.status, mi_plan_status(s->solver), C.X.status);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
+// Before a driver-loop run: the device cadence takes the host's changes.
+int mi_before_run(gamera_cs_mi_dipole *s) { return push_cadence(s); }
+
+// After a driver-loop run: the host copies are refreshed on next access.
+void mi_after_run(gamera_cs_mi_dipole *s) { s->stale = 1; }
+
+// The device potential of a coupling updated inside context C's step graph
+// (the Earth boundary reads it directly), else null.
+const double *mi_graph_potential(const gamera_cs_mi_dipole *s, const Context *C) {
+  return s != nullptr && s->in_graph && s->ctx == C && C->mi_graph == s ? s->d_pot
+                                                                        : nullptr;
+}
+
+// Lookup parameters of a coupling updated inside context C's step graph,
+// with the potential pointing at its device copy: every step's update runs
+// before the step reads it, so the wall uses the coupling from the first
+// step on.
+bool mi_lookup_device(const gamera_cs_mi_dipole *s, const Context *C, MiLookup *L,
+                      double *potential_norm_v) {
+  const double *d = mi_graph_potential(s, C);
+  if (d == nullptr) return false;
+  *L = lookup_of(s);
+  L->pot[0] = d;
+  L->pot[1] = d + (size_t)s->np * s->nt;
+  *potential_norm_v = s->potential_norm_v;
+  return true;
+}
+
+}  // namespace gcs
+
+extern "C" {
+
+int gcs_context_set_mi_coupling(gcs_context *ctx, gamera_cs_mi_dipole *mi,
+                                int every_steps) {
+  gcs::Context *C = gcs::context_of(ctx);
+  if (C == nullptr || every_steps < 0) {
+    set_api_error("invalid MI coupling attachment");
+    return -1;
+  }
+  if (C->mi_graph != nullptr) {
+    gamera_cs_mi_dipole *old = C->mi_graph;
+    if (sync_host(old) != 0) return -1;
+    old->in_graph = 0;
+    C->mi_graph = nullptr;
+  }
+  if (mi == nullptr) return 0;
+  if (mi->ctx != C || mi->d_cad == nullptr) {
+    set_api_error("the MI coupling belongs to another context");
+    return -1;
+  }
+  if (sync_host(mi) != 0) return -1;
+  mi->every = every_steps;
+  mi->in_graph = 1;
+  mi->push = 1;
+  if (push_cadence(mi) != 0) return -1;
+  C->mi_graph = mi;
+  return 0;
 }
 
 }  // extern "C"

@@ -145,5 +145,10 @@ GCS_HD inline int mi_ghost_velocity(const MiLookup &L, gamera_no_vec3 point,
 // The lookup parameters and host potential of a ready coupling
 // (gcs_mi_dipole.cu); false when it is not ready.
 bool mi_lookup(const ::gamera_cs_mi_dipole *s, MiLookup *L, double *potential_norm_v);
+// The same for a coupling updated inside context C's step graph, with the
+// potential on the device; false otherwise (gcs_mi_dipole.cu).
+struct Context;
+bool mi_lookup_device(const ::gamera_cs_mi_dipole *s, const Context *C, MiLookup *L,
+                      double *potential_norm_v);
 
 }  // namespace gcs

@@ -239,7 +239,8 @@ enum {
   GCS_STAGE_SOLVE_EDGE = 17,
   GCS_STAGE_OPTIONS = 18,
   GCS_STAGE_PRESSURE_CONTROL = 19,
-  GCS_STAGE_TILE_COPY = 20
+  GCS_STAGE_TILE_COPY = 20,
+  GCS_STAGE_MI_COUPLING = 21
 };
 
 /* Build a device context from a host grid in the reference layout
@@ -308,6 +309,9 @@ int gcs_context_run(gcs_context *ctx, const gamera_no_advance_options *options,
                     const gamera_no_timestep_options *timestep,
                     double dt_fraction, int steps, int use_graph);
 int gcs_context_sync(gcs_context *ctx);
+/* Simulation time (code units) of the state in the device driver loop: the
+ * sum of the time steps gcs_context_run has taken. */
+int gcs_context_time(gcs_context *ctx, double *time);
 int gcs_context_params(gcs_context *ctx, double *dt, double *ratio,
                        double *cfl_min, int *steps);
 int gcs_context_set_params(gcs_context *ctx, double dt, double ratio,
@@ -673,6 +677,20 @@ int gcs_mi_tensor_results(gcs_mi_tensor_plan *plan, gamera_mi_solver_stats *stat
 int gcs_context_mi_dipole_create(gcs_context *ctx, const gamera_cs_earth_startup *startup,
                                  const gamera_cs_mi_dipole_config *config,
                                  gamera_cs_mi_dipole **result);
+/* The coupling update inside the device driver loop (gcs_context_run,
+ * gcs_context_run_earth): before every step the step's CUDA graph
+ * evaluates the coupling's cadence on the device and, when it is due, runs
+ * the FAC kernels and both hemisphere solves, with no host round trip.
+ * every_steps = 0 keeps the reference's rule on the simulation time of the
+ * state (cubedsphere_mi_dipole.c:372-378, gamera_cs_mi_dipole_maybe_update
+ * with the driver's time); every_steps = n updates before every n-th step
+ * (and before the first).  A failed update fails the step (stage
+ * GCS_STAGE_MI_COUPLING).  An Earth boundary with this coupling as its MI
+ * wall reads the potential on the device.  The coupling's host entry points
+ * see the device's state after the run.  The caller does not also call
+ * gamera_cs_mi_dipole_maybe_update for steps run this way.  mi = NULL
+ * detaches.  No reference counterpart. */
+int gcs_context_set_mi_coupling(gcs_context *ctx, gamera_cs_mi_dipole *mi, int every_steps);
 int gcs_mi_plan_create(const gamera_mi_solver_config *configs, int count,
                        gcs_mi_plan **plan);
 void gcs_mi_plan_destroy(gcs_mi_plan *plan);

@@ -83,9 +83,12 @@ def test_in_graph_cadence_matches_host_driven(lib, every):
             if every == 0:
                 rc = lib.gamera_cs_mi_dipole_maybe_update(ma, _time(lib, a))
             elif s % every == 0:
-                # the host-driven form of an every-n-steps cadence: each
-                # update forced by a time far beyond the next update
-                rc = lib.gamera_cs_mi_dipole_maybe_update(ma, 1e9 * (s + 1))
+                # the host-driven form of an every-n-steps cadence: the k-th
+                # update at the time of the k-th coupling interval, where the
+                # reference's rule makes it due
+                rc = lib.gamera_cs_mi_dipole_maybe_update(
+                    ma, updates * cfg.coupling_interval_s * cfg.speed_norm_m_s /
+                    cfg.length_norm_m)
             else:
                 rc = 0
             assert rc in (0, 1), lib.gcs_last_error()

@@ -345,6 +345,7 @@ def run_gpu(args):
     lib.gcs_context_destroy(ctx)
     ctx = None
     ens = run_ensemble(lib, torch, device, args, dist, rank) if args.ens_steps > 0 else None
+    c3 = run_c3(lib, args) if args.c3_steps > 0 else None
 
     result = None
     if rank == 0:
@@ -417,6 +418,8 @@ def run_gpu(args):
             result["fp32_bulk"] = bulk
         if ens is not None:
             result["ensemble"] = ens
+        if c3 is not None:
+            result["fp32_bulk_c3"] = c3
         if earth is not None:
             result["earth_boundary"] = earth
         if args.cpu_baseline and world == 1:
@@ -472,6 +475,21 @@ def run_bulk(lib, torch, device, args, dist):
             "note": "flux/face-velocity/EMF sweeps in FP32 outside the layers "
                     "where |B0| > 8 (those stay FP64); state, face B, CT, "
                     "predictor and recovery FP64"}
+
+
+def run_c3(lib, args):
+    """Precision configuration 6 x 192x192x384 (84.9 M cells): the wind with
+    a seeded 20 % sinusoidal density pulse of wavelength 10 R_E
+    (V = -450 km/s, n = 5 cm^-3, Bz = -5 nT), args.c3_steps steps of the
+    FP32-bulk path against the FP64 path on the same time levels, one
+    context on the GPU at a time; per-variable L2/Linf relative errors and
+    max |div B| of both, and both wall times per step."""
+    from gamera_cube_b200 import precision
+    r = precision.compare_bulk_sequential(lib, 3, 384, 192, args.c3_steps, seed=1000)
+    r["workload"] = ("6 x 192x192x384 wind + dipole with a 20% density pulse "
+                     "(lambda 10 R_E, V = -450 km/s)")
+    r["max_rel_linf"] = max(r[v]["linf"] for v in precision.VARIABLES)
+    return r
 
 
 def run_earth(lib, torch, device, args, dist, ctx):
@@ -986,6 +1004,10 @@ def main():
     ap.add_argument("--ens-steps", type=int, default=20,
                     help="timed steps of the 16-run ensemble (0 skips it)")
     ap.add_argument("--ens-warmup", type=int, default=3)
+    ap.add_argument("--c3-steps", type=int, default=0,
+                    help="steps of the 6 x 192x192x384 density-pulse precision run "
+                         "(FP32-bulk against FP64 on the same time levels; about "
+                         "5 minutes for 1000 steps, so off by default)")
     ap.add_argument("--only-mi", action="store_true",
                     help="run only the standalone ionosphere solve measurement "
                          "(prints its JSON object; for profiling)")

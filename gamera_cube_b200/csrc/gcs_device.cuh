@@ -82,8 +82,21 @@ struct DevBg {
 // outputs, which are FP64 in both paths.  Bulk<double> views the FP64
 // arrays of DevState/DevGeom/DevBg; Bulk<float> views separate FP32 copies
 // (FP32-bulk path) and the same FP64 outputs.
+//
+// The FP32 arrays cover only the radial layers [lo, N0) of each face (the
+// layers the FP32 sweeps read), six faces of face_nodes = (N0 - lo) N1 N2
+// nodes each: a node of face f sits at at(f, node) = f face_nodes + node -
+// lo N1 N2.  The FP64 view has lo = 0, face_nodes = Nn, so at() is the
+// node index of the full arrays.  The sweep outputs (FV, F, M, E) are the
+// full FP64 arrays in both views and keep the full index.
 template <typename T>
 struct Bulk {
+  int lo;                    // first radial layer of the arrays of this view
+  long long face_nodes;      // nodes per face of this view's arrays
+  long long shift;           // lo * N1 * N2
+  GCS_HD long long at(int f, long long node) const {
+    return (long long)f * face_nodes + node - shift;
+  }
   T *Pr[5], *Bp[3], *BN[3], *W[3];
   double *FV[3][3], *F[3][5], *M[3][3], *E[3];
   const T *vol, *iv[3], *area[3];

@@ -126,14 +126,16 @@ __device__ __forceinline__ TileCoord tile_coord(const FluxTiles &L, long long t)
 }
 
 // One elected thread: copies of tile t's staged cells into stage buffer sm.
+// The cell arrays of the view cover layers [lo, N0) of each face, so the
+// tensor's third coordinate is face * (N0 - lo) + i - lo.
 template <int d, typename T>
 __device__ __forceinline__ void issue_tile(const FluxMaps &maps, const Dims &D,
                                            const FluxTiles &L, long long t, T *sm,
-                                           unsigned long long *bar) {
+                                           unsigned long long *bar, int lo) {
   using S = FluxTile<d, T>;
   const TileCoord c = tile_coord<d, T>(L, t);
   int x, y, z;
-  const int zf = c.f * (D.E0 + 1);
+  const int zf = c.f * (D.E0 + 1 - lo) - lo;
   if (d == 0) {
     x = D.g + c.b;
     y = c.row;
@@ -169,8 +171,9 @@ __device__ __forceinline__ void staged_face(const T *sm, int s0, const Dims &D,
                                             int j, int k) {
   using Sh = FluxTile<d, T>;
   const long long c = f * D.Nn + D.node(i, j, k);
+  const long long cb = B.at(f, D.node(i, j, k));   // index of the Bulk arrays
   const long long sd = D.stride(d);
-  const T iv = B.iv[d][c];
+  const T iv = B.iv[d][cb];
   if (isnan(iv)) {
     fail(st, kStageReconstruct, d, f, i, j, k);
     return;
@@ -230,9 +233,9 @@ __device__ __forceinline__ void staged_face(const T *sm, int s0, const Dims &D,
     }
   }
   FaceFrame<T> fr;
-  fr.nx = B.fn[d][0][c]; fr.ny = B.fn[d][1][c]; fr.nz = B.fn[d][2][c];
-  fr.t1x = B.ft1[d][0][c]; fr.t1y = B.ft1[d][1][c]; fr.t1z = B.ft1[d][2][c];
-  fr.t2x = B.ft2[d][0][c]; fr.t2y = B.ft2[d][1][c]; fr.t2z = B.ft2[d][2][c];
+  fr.nx = B.fn[d][0][cb]; fr.ny = B.fn[d][1][cb]; fr.nz = B.fn[d][2][cb];
+  fr.t1x = B.ft1[d][0][cb]; fr.t1y = B.ft1[d][1][cb]; fr.t1z = B.ft1[d][2][cb];
+  fr.t2x = B.ft2[d][0][cb]; fr.t2y = B.ft2[d][1][cb]; fr.t2z = B.ft2[d][2][cb];
   FluidFlux<T> fl;
   if (kinetic_fluid_flux(st2, (T)O.s_gamma, fr, &fl)) {
     fail(st, kStageKineticFluid, d, f, i, j, k);
@@ -241,14 +244,14 @@ __device__ __forceinline__ void staged_face(const T *sm, int s0, const Dims &D,
   MaxwellFlux<T> mx;
   mx.m[0] = mx.m[1] = mx.m[2] = T(0.0);
   if (O.s_mhd) {
-    const T bn = B.BN[d][c];
+    const T bn = B.BN[d][cb];
     T b0[3] = {T(0.0), T(0.0), T(0.0)};
     T b0n = T(0.0);
     if (O.s_bg) {
-      b0[0] = B.fb0[d][0][c];
-      b0[1] = B.fb0[d][1][c];
-      b0[2] = B.fb0[d][2][c];
-      b0n = B.fb0n[d][c];
+      b0[0] = B.fb0[d][0][cb];
+      b0[1] = B.fb0[d][1][cb];
+      b0[2] = B.fb0[d][2][cb];
+      b0n = B.fb0n[d][cb];
     }
     if (kinetic_maxwell_flux(st2, mag, bn, fr, O.s_bg, b0, b0n, O.s_boris, (T)O.s_c,
                              fl.vn, &mx)) {
@@ -271,7 +274,7 @@ __device__ __forceinline__ void staged_face(const T *sm, int s0, const Dims &D,
       }
     }
   }
-  const T area = B.area[d][c];
+  const T area = B.area[d][cb];
 #pragma unroll
   for (int m = 0; m < 5; ++m) B.F[d][m][c] = (double)(area * fl.f[m]);
 #pragma unroll
@@ -340,7 +343,7 @@ __global__ void __launch_bounds__(256, FluxTile<d, T>::MIN_BLOCKS)
       for (int q = 0; q < Sh::STAGES; ++q)
         if (first + q * stride < L.count)
           issue_tile<d, T>(maps, D, L, first + q * stride,
-                           (T *)(base + q * Sh::STAGE_BYTES), &full[q]);
+                           (T *)(base + q * Sh::STAGE_BYTES), &full[q], B.lo);
     }
   }
   __syncthreads();
@@ -396,17 +399,19 @@ __global__ void __launch_bounds__(256, FluxTile<d, T>::MIN_BLOCKS)
         const long long next = t + (long long)Sh::STAGES * stride;
         if (next < L.count) {
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          issue_tile<d, T>(maps, D, L, next, (T *)(base + s * Sh::STAGE_BYTES), &full[s]);
+          issue_tile<d, T>(maps, D, L, next, (T *)(base + s * Sh::STAGE_BYTES), &full[s],
+                           B.lo);
         }
       }
     }
   }
 }
 
-// Host: tensor map of one FP64 or FP32 node array (all six faces viewed as
-// the 3-D tensor k x j x (face, i)) with the given box (gcs_setup.cu).
+// Host: tensor map of one FP64 or FP32 node array (all six faces, layers
+// [lo, N0) of each, viewed as the 3-D tensor k x j x (face, i)) with the
+// given box (gcs_setup.cu).
 int encode_cell_map(CUtensorMap *map, const void *base, int elem_bytes, const Dims &D,
-                    int box_x, int box_y, int box_z);
+                    int lo, int box_x, int box_y, int box_z);
 // Host: record a failure of the step at a stage (gcs_kernels.cu).
 void launch_set_failure(const Ctx &X, int stage, int dir, cudaStream_t s);
 
@@ -488,7 +493,7 @@ void launch_flux_tma(const Ctx &X, const Bulk<T> &B, const Opts &O, int i0, int 
   const void *arrays[9] = {B.Pr[0], B.Pr[1], B.Pr[2], B.Pr[3], B.Pr[4],
                            B.Bp[0], B.Bp[1], B.Bp[2], B.vol};
   for (int v = 0; v < 9; ++v)
-    if (encode_cell_map(&maps.m[v], arrays[v], (int)sizeof(T), D, Sh::BX, Sh::BY,
+    if (encode_cell_map(&maps.m[v], arrays[v], (int)sizeof(T), D, B.lo, Sh::BX, Sh::BY,
                         Sh::BZ) != 0) {
       // no sweep without its tensor maps: the step fails at this stage
       launch_set_failure(X, kStageTileCopy, d, s);

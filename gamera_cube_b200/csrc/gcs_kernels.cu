@@ -344,6 +344,9 @@ __global__ void k_count_step(StepParams *prm) {
 
 Bulk<double> bulk64(const Ctx &X) {
   Bulk<double> B{};
+  B.lo = 0;
+  B.face_nodes = X.D.Nn;
+  B.shift = 0;
   const DevState &S = X.S;
   const DevGeom &G = X.G;
   const DevBg &BG = X.BG;

@@ -869,9 +869,14 @@ namespace gcs {
 
 namespace {
 
-__global__ void k_to_f32(const double *src, float *dst, long long n) {
+// FP32 copy of the layers [lo, N0) of every face of a full FP64 node array
+// (the window of the FP32-bulk arrays, Bulk::at).
+__global__ void k_to_f32_window(const double *src, float *dst, long long face_nodes,
+                                long long Nn, long long shift) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) dst[t] = (float)src[t];
+  if (t >= kFaces * face_nodes) return;
+  const long long f = t / face_nodes;
+  dst[t] = (float)src[f * Nn + shift + (t - f * face_nodes)];
 }
 
 __global__ void k_layer_b0(Dims D, DevBg BG, unsigned long long *layer_max) {
@@ -911,8 +916,18 @@ int Context::enable_bulk(int on) {
     X.bulk = 0;
     return 0;
   }
-  const long long n = (long long)kFaces * X.D.Nn;
   const int arrays = 14 + 76 + 18;
+  if (!bulk_pool) {
+    // the FP32 arrays cover the layers the FP32 sweeps read: from four
+    // layers (the Up7 reach) inside the first FP32 layer outwards
+    if (set_bulk_split(bulk_b0_threshold) != 0) return -1;
+    const Dims &D = X.D;
+    const int lo = X.bulk_split > 4 ? X.bulk_split - 4 : 0;
+    X.B32.lo = lo;
+    X.B32.face_nodes = (long long)(D.E0 + 1 - lo) * D.N1 * D.N2;
+    X.B32.shift = (long long)lo * D.N1 * D.N2;
+  }
+  const long long n = (long long)kFaces * X.B32.face_nodes;
   if (!bulk_pool) {
     bulk_bytes = (size_t)arrays * n * sizeof(float);
     if (cudaMalloc(&bulk_pool, bulk_bytes) != cudaSuccess) {
@@ -943,7 +958,8 @@ int Context::enable_bulk(int on) {
     const unsigned nb = (unsigned)((n + bs - 1) / bs);
     auto conv = [&](const double *src) -> const float * {
       float *dst = take();
-      if (src) k_to_f32<<<nb, bs, 0, stream>>>(src, dst, n);
+      if (src)
+        k_to_f32_window<<<nb, bs, 0, stream>>>(src, dst, B.face_nodes, X.D.Nn, B.shift);
       return dst;
     };
     B.vol = conv(G.vol);
@@ -981,7 +997,9 @@ int Context::enable_bulk(int on) {
     const int bs = 256;
     const unsigned nb = (unsigned)((n + bs - 1) / bs);
     auto conv = [&](const double *src, const float *dst) {
-      if (src) k_to_f32<<<nb, bs, 0, stream>>>(src, (float *)dst, n);
+      if (src)
+        k_to_f32_window<<<nb, bs, 0, stream>>>(src, (float *)dst, B.face_nodes, X.D.Nn,
+                                               B.shift);
     };
     for (int d = 0; d < 3; ++d) {
       conv(BG.fb0n[d], B.fb0n[d]);
@@ -1036,6 +1054,18 @@ int Context::set_bulk_split(double b0_threshold) {
       break;
     }
   }
+  if (bulk_pool != nullptr && X.bulk_split - 4 < X.B32.lo) {
+    // the FP32 window no longer reaches the new first FP32 layer: rebuild
+    // the FP32 arrays for the wider window
+    cudaStreamSynchronize(stream);
+    cudaFree(bulk_pool);
+    bulk_pool = nullptr;
+    bulk_bytes = 0;
+    X.B32 = Bulk<float>{};
+    const int was = X.bulk;
+    X.bulk = 0;
+    if (was) return enable_bulk(1);
+  }
   return 0;
 }
 
@@ -1043,12 +1073,13 @@ int Context::set_bulk_split(double b0_threshold) {
 
 namespace gcs {
 
-// Tensor map of one node array of all six faces, viewed as the 3-D tensor
-// (k: N2, j: N1, face * N0 + i: 6 N0) with k contiguous, for the TMA-staged
+// Tensor map of one node array of all six faces (layers [lo, N0) of each),
+// viewed as the 3-D tensor (k: N2, j: N1, face * (N0 - lo) + i - lo) with k
+// contiguous, for the TMA-staged
 // sweeps.  The driver's encoder is reached through the runtime's entry-point
 // query, so the library links the runtime only.
 int encode_cell_map(CUtensorMap *map, const void *base, int elem_bytes, const Dims &D,
-                    int box_x, int box_y, int box_z) {
+                    int lo, int box_x, int box_y, int box_z) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (encode == nullptr) {
     void *fn = nullptr;
@@ -1061,7 +1092,7 @@ int encode_cell_map(CUtensorMap *map, const void *base, int elem_bytes, const Di
   }
   if (((size_t)base & 15) != 0 || (elem_bytes != 4 && elem_bytes != 8)) return -1;
   const cuuint64_t dims[3] = {(cuuint64_t)D.N2, (cuuint64_t)D.N1,
-                              (cuuint64_t)kFaces * (cuuint64_t)(D.E0 + 1)};
+                              (cuuint64_t)kFaces * (cuuint64_t)(D.E0 + 1 - lo)};
   const cuuint64_t strides[2] = {(cuuint64_t)D.N2 * elem_bytes,
                                  (cuuint64_t)D.N2 * D.N1 * elem_bytes};
   const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_z};

@@ -45,6 +45,9 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const double r = prm->ratio;
   const long long c = f * D.Nn + D.node(i, j, k);
+  // FP32 copies exist for the layers [B32.lo, N0) only
+  const bool wb = bulk && i >= B32.lo;
+  const long long cb = wb ? B32.at(f, D.node(i, j, k)) : 0;
   const bool cell = i < D.E0 && j < D.E1 && k < D.E2;
   const int coord[3] = {i, j, k};
 #pragma unroll
@@ -57,7 +60,7 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
       S.Pp[d][c] = pp;
       const double bn = pp / G.area[d][c];
       S.BN[d][c] = bn;
-      if (bulk) B32.BN[d][c] = (float)bn;
+      if (wb) B32.BN[d][cb] = (float)bn;
     }
   }
   if (!cell) return;
@@ -79,7 +82,7 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
     S.Pr[m][c] = prv[m];
-    if (bulk) B32.Pr[m][c] = (float)prv[m];
+    if (wb) B32.Pr[m][cb] = (float)prv[m];
   }
   const double v = G.vol[c];
   const double rho = fmax(up[0], O.e_rho_floor);
@@ -87,7 +90,7 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
   for (int m = 0; m < 3; ++m) {
     const double w = v * up[1 + m] / rho;
     S.W[m][c] = w;
-    if (bulk) B32.W[m][c] = (float)w;
+    if (wb) B32.W[m][cb] = (float)w;
   }
   double phi[6];
 #pragma unroll
@@ -104,7 +107,7 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     S.Bp[m][c] = bp[m];
-    if (bulk) B32.Bp[m][c] = (float)bp[m];
+    if (wb) B32.Bp[m][cb] = (float)bp[m];
   }
 }
 #endif  // GCS_SWEEPS_TEMPLATES_ONLY
@@ -137,8 +140,9 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, D
   const Box b{i0, D.g, D.g, D.n + (d == 1), D.n + (d == 2), i1};
   if (!box_coord(b, &f, &i, &j, &k)) return;
   const long long c = f * D.Nn + D.node(i, j, k);
+  const long long cb = B.at(f, D.node(i, j, k));   // index of the Bulk arrays
   const long long sd = D.stride(d);
-  const T iv = B.iv[d][c];
+  const T iv = B.iv[d][cb];
   if (isnan(iv)) {
     fail(st, kStageReconstruct, d, f, i, j, k);
     return;
@@ -147,14 +151,14 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, D
   const T pdm = (T)O.pdm;
   T vol[8];
 #pragma unroll
-  for (int n = 0; n < 8; ++n) vol[n] = B.vol[c + (n - 4) * sd];
+  for (int n = 0; n < 8; ++n) vol[n] = B.vol[cb + (n - 4) * sd];
   PrimT<T> st2[2];
   {
     T q[8], l, r;
     bool ok = true;
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
-      q[n] = B.Pr[0][c + (n - 4) * sd];
+      q[n] = B.Pr[0][cb + (n - 4) * sd];
       ok = ok && !isnan(q[n]);
     }
     if (!ok) {
@@ -164,19 +168,19 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, D
     up7_pdm_rcp(vol, q, riv, pdm, &l, &r);
     st2[0].rho = l; st2[1].rho = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = B.Pr[1][c + (n - 4) * sd];
+    for (int n = 0; n < 8; ++n) q[n] = B.Pr[1][cb + (n - 4) * sd];
     up7_pdm_rcp(vol, q, riv, pdm, &l, &r);
     st2[0].vx = l; st2[1].vx = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = B.Pr[2][c + (n - 4) * sd];
+    for (int n = 0; n < 8; ++n) q[n] = B.Pr[2][cb + (n - 4) * sd];
     up7_pdm_rcp(vol, q, riv, pdm, &l, &r);
     st2[0].vy = l; st2[1].vy = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = B.Pr[3][c + (n - 4) * sd];
+    for (int n = 0; n < 8; ++n) q[n] = B.Pr[3][cb + (n - 4) * sd];
     up7_pdm_rcp(vol, q, riv, pdm, &l, &r);
     st2[0].vz = l; st2[1].vz = r;
 #pragma unroll
-    for (int n = 0; n < 8; ++n) q[n] = B.Pr[4][c + (n - 4) * sd];
+    for (int n = 0; n < 8; ++n) q[n] = B.Pr[4][cb + (n - 4) * sd];
     up7_pdm_rcp(vol, q, riv, pdm, &l, &r);
     st2[0].p = l; st2[1].p = r;
   }
@@ -186,14 +190,14 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, D
     for (int m = 0; m < 3; ++m) {
       T q[8];
 #pragma unroll
-      for (int n = 0; n < 8; ++n) q[n] = B.Bp[m][c + (n - 4) * sd];
+      for (int n = 0; n < 8; ++n) q[n] = B.Bp[m][cb + (n - 4) * sd];
       up7_pdm_rcp(vol, q, riv, pdm, &mag[0][m], &mag[1][m]);
     }
   }
   FaceFrame<T> fr;
-  fr.nx = B.fn[d][0][c]; fr.ny = B.fn[d][1][c]; fr.nz = B.fn[d][2][c];
-  fr.t1x = B.ft1[d][0][c]; fr.t1y = B.ft1[d][1][c]; fr.t1z = B.ft1[d][2][c];
-  fr.t2x = B.ft2[d][0][c]; fr.t2y = B.ft2[d][1][c]; fr.t2z = B.ft2[d][2][c];
+  fr.nx = B.fn[d][0][cb]; fr.ny = B.fn[d][1][cb]; fr.nz = B.fn[d][2][cb];
+  fr.t1x = B.ft1[d][0][cb]; fr.t1y = B.ft1[d][1][cb]; fr.t1z = B.ft1[d][2][cb];
+  fr.t2x = B.ft2[d][0][cb]; fr.t2y = B.ft2[d][1][cb]; fr.t2z = B.ft2[d][2][cb];
   FluidFlux<T> fl;
   if (kinetic_fluid_flux(st2, (T)O.s_gamma, fr, &fl)) {
     fail(st, kStageKineticFluid, d, f, i, j, k);
@@ -202,14 +206,14 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, D
   MaxwellFlux<T> mx;
   mx.m[0] = mx.m[1] = mx.m[2] = T(0.0);
   if (O.s_mhd) {
-    const T bn = B.BN[d][c];
+    const T bn = B.BN[d][cb];
     T b0[3] = {T(0.0), T(0.0), T(0.0)};
     T b0n = T(0.0);
     if (O.s_bg) {
-      b0[0] = B.fb0[d][0][c];
-      b0[1] = B.fb0[d][1][c];
-      b0[2] = B.fb0[d][2][c];
-      b0n = B.fb0n[d][c];
+      b0[0] = B.fb0[d][0][cb];
+      b0[1] = B.fb0[d][1][cb];
+      b0[2] = B.fb0[d][2][cb];
+      b0n = B.fb0n[d][cb];
     }
     if (kinetic_maxwell_flux(st2, mag, bn, fr, O.s_bg, b0, b0n, O.s_boris, (T)O.s_c,
                              fl.vn, &mx)) {
@@ -232,7 +236,7 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::flux) k_flux(Dims D, D
       }
     }
   }
-  const T area = B.area[d][c];
+  const T area = B.area[d][cb];
 #pragma unroll
   for (int m = 0; m < 5; ++m) B.F[d][m][c] = (double)(area * fl.f[m]);
 #pragma unroll
@@ -294,13 +298,14 @@ __global__ void k_face_velocity(Dims D, Bulk<T> B, DevStatus *st, int i0,
   const Box b{i0, lo[1], lo[2], cnt[1], cnt[2], i1};
   if (!box_coord(b, &f, &x[0], &x[1], &x[2])) return;
   const long long c = f * D.Nn + D.node(x[0], x[1], x[2]);
+  const long long cb = B.at(f, D.node(x[0], x[1], x[2]));
   const long long sa = D.stride(a);
-  const T riv = T(1.0) / B.iv[a][c];
+  const T riv = T(1.0) / B.iv[a][cb];
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     T w[8];
 #pragma unroll
-    for (int n = 0; n < 8; ++n) w[n] = B.W[m][c + (n - 4) * sa];
+    for (int n = 0; n < 8; ++n) w[n] = B.W[m][cb + (n - 4) * sa];
     B.FV[a][m][c] = (double)(central8(w) * riv);
   }
 }
@@ -323,6 +328,7 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::edge) k_edge_emf(Dims 
   const Box b{i0, D.g, D.g, cnt[1], cnt[2], i1};
   if (!box_coord(b, &f, &x[0], &x[1], &x[2])) return;
   const long long c = f * D.Nn + D.node(x[0], x[1], x[2]);
+  const long long cb = B.at(f, D.node(x[0], x[1], x[2]));
   const unsigned char ok = G.edge_ok[e][c];
   if (ok != 0) {
     fail(st, ok, e, f, x[0], x[1], x[2]);
@@ -334,8 +340,8 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::edge) k_edge_emf(Dims 
   T ar[8], fld[8];
   T v[3];
 #pragma unroll
-  for (int n = 0; n < 8; ++n) ar[n] = B.area[a][c + (n - 4) * sb];
-  const T rca = T(1.0) / B.ca[e][c];
+  for (int n = 0; n < 8; ++n) ar[n] = B.area[a][cb + (n - 4) * sb];
+  const T rca = T(1.0) / B.ca[e][cb];
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     T w[8];
@@ -343,31 +349,31 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::edge) k_edge_emf(Dims 
     for (int n = 0; n < 8; ++n) w[n] = ar[n] * (T)B.FV[a][m][c + (n - 4) * sb];
     v[m] = central8(w) * rca;
   }
-  const T vt1 = dot3(v[0], v[1], v[2], B.et1[e][0][c], B.et1[e][1][c], B.et1[e][2][c]);
-  const T vt2 = dot3(v[0], v[1], v[2], B.et2[e][0][c], B.et2[e][1][c], B.et2[e][2][c]);
+  const T vt1 = dot3(v[0], v[1], v[2], B.et1[e][0][cb], B.et1[e][1][cb], B.et1[e][2][cb]);
+  const T vt2 = dot3(v[0], v[1], v[2], B.et2[e][0][cb], B.et2[e][1][cb], B.et2[e][2][cb]);
   // transverse face fields (nonorthogonal_sweep.c:372-406)
   T fl, fr, sl, sr;
 #pragma unroll
-  for (int n = 0; n < 8; ++n) fld[n] = B.BN[a][c + (n - 4) * sb];
+  for (int n = 0; n < 8; ++n) fld[n] = B.BN[a][cb + (n - 4) * sb];
   up7_pdm_rcp(ar, fld, rca, pdm, &fl, &fr);
   T ar2[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
-    ar2[n] = B.area[bb][c + (n - 4) * sa];
-    fld[n] = B.BN[bb][c + (n - 4) * sa];
+    ar2[n] = B.area[bb][cb + (n - 4) * sa];
+    fld[n] = B.BN[bb][cb + (n - 4) * sa];
   }
-  up7_pdm_rcp(ar2, fld, T(1.0) / B.cb[e][c], pdm, &sl, &sr);
+  up7_pdm_rcp(ar2, fld, T(1.0) / B.cb[e][cb], pdm, &sl, &sr);
   // 2x2 edge solve (nonorthogonal_operators.c:56-79)
   const T f1 = T(0.5) * (fl + fr);
   const T f2 = T(0.5) * (sl + sr);
-  const T inv = B.einv[e][c];
-  const T n10 = B.en1[e][0][c], n11 = B.en1[e][1][c];
-  const T n20 = B.en2[e][0][c], n21 = B.en2[e][1][c];
+  const T inv = B.einv[e][cb];
+  const T n10 = B.en1[e][0][cb], n11 = B.en1[e][1][cb];
+  const T n20 = B.en2[e][0][cb], n21 = B.en2[e][1][cb];
   T ef0 = inv * (n21 * f1 - n11 * f2);
   T ef1 = inv * (-n20 * f1 + n10 * f2);
   if (O.e_bg) {
-    ef0 += B.eb0t1[e][c];
-    ef1 += B.eb0t2[e][c];
+    ef0 += B.eb0t1[e][cb];
+    ef1 += B.eb0t2[e][cb];
   }
   const T jump = (sr - sl) - (fr - fl);
   // edge density (nonorthogonal_sweep.c:351-370), from the FP64 state
@@ -381,7 +387,7 @@ __global__ void __launch_bounds__(128, SweepOccupancy<T>::edge) k_edge_emf(Dims 
     return;
   }
   T emf;
-  if (edge_emf(vt1, vt2, ef0, ef1, jump, (T)rho, B.elen[e][c], (T)O.e_diff, O.e_boris,
+  if (edge_emf(vt1, vt2, ef0, ef1, jump, (T)rho, B.elen[e][cb], (T)O.e_diff, O.e_boris,
                (T)O.e_c, (T)O.e_cfl, (T)prm->dt, &emf)) {
     fail(st, kStageEdgeEmf, e, f, x[0], x[1], x[2]);
     return;

@@ -2,7 +2,10 @@
 (cubedsphere/cubedsphere_analysis_hdf5.c:316-331 with
 nonorthogonal_state.c:60-93): per face float32 [8][NI][NJ][NK] of rho, p,
 vx, vy, vz from the conserved state (floors 1e-12) and the total B
-(residual + cell B0) over the active cells.  Test infrastructure only."""
+(residual + cell B0) over the active cells.  Test infrastructure only.
+Pinned bit for bit to frames recorded through the reference library's own
+gamera_no_conserved_to_primitive (tests/golden/make_analysis_golden.py,
+tests/test_analysis_oracle.py)."""
 import numpy as np
 
 

@@ -53,6 +53,11 @@ def test_frame_matches_restatement(lib):
         assert lib.gcs_context_analysis_frame(ctx, GAMMA, None, host.ctypes.data) == 0
         want = expected(case)
         np.testing.assert_array_equal(host.reshape(want.shape), want)
+        # and the frames recorded through the reference's own conversion
+        # (tests/golden/make_analysis_golden.py, same case and step)
+        golden = np.load(os.path.join(os.path.dirname(__file__), "golden",
+                                      "reference_analysis.npz"))["frames"]
+        np.testing.assert_array_equal(host.reshape(golden.shape), golden)
         # an invalid state fails as the reference writer does
         case.arrays(3)["conserved"][6, 7, 8, 0] = -1.0
         assert lib.gcs_context_upload_state(ctx, case.storage) == 0

@@ -209,6 +209,8 @@ def run_gpu(args):
     if not ctx:
         raise RuntimeError(lib.gcs_last_error().decode())
     setup_s = time.time() - t0
+    if args.flux_staging and lib.gcs_context_set_flux_staging(ctx, 1) != 0:
+        raise RuntimeError("flux staging rejected")
     opts, ts = abi.AdvanceOptions(), abi.TimestepOptions()
     lib.gcs_case_options(KIND_WIND, C.byref(opts), C.byref(ts))
     stream = torch.cuda.ExternalStream(lib.gcs_context_stream(ctx), device=device)
@@ -411,6 +413,7 @@ def run_gpu(args):
                          "step_hbm_frac": cells * STEP_BYTES_PER_CELL /
                          (ms_local / args.steps * 1e-3) / 1e9 / hbm},
             "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+            "flux_sweep": "TMA-staged" if args.flux_staging else "per-face",
         }
         if mi_solo is not None:
             result["mi"] = mi_solo
@@ -1004,6 +1007,9 @@ def main():
     ap.add_argument("--ens-steps", type=int, default=20,
                     help="timed steps of the 16-run ensemble (0 skips it)")
     ap.add_argument("--ens-warmup", type=int, default=3)
+    ap.add_argument("--flux-staging", action="store_true",
+                    help="use the TMA-staged flux sweep (gcs_context_set_flux_staging) "
+                         "instead of the default per-face sweep")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="steps of the 6 x 192x192x384 density-pulse precision run "
                          "(FP32-bulk against FP64 on the same time levels; about "

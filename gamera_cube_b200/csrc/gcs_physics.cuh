@@ -2,8 +2,10 @@
 //
 // Every function restates one reference operator with the same operation
 // order (so the FP64 path tracks the CPU reference to round-off); the cited
-// lines are in the GAMERA-Cube project.  Functions return 0 on success and a
-// nonzero value where the reference returns -1.
+// lines are in the GAMERA-Cube project.  The exceptions are marked where they
+// occur: a repeated divisor applied as one reciprocal, sqrt(pi lambda) taken
+// as sqrt(pi) sqrt(lambda), each a change in the last bit.  Functions return
+// 0 on success and a nonzero value where the reference returns -1.
 #pragma once
 
 #include <cfloat>
@@ -241,7 +243,11 @@ __device__ inline int kinetic_fluid_flux(const PrimT<T> st[2], T gamma,
     fl->jump[m] = T(0.0);
   }
   fl->vjump[0] = fl->vjump[1] = fl->vjump[2] = T(0.0);
-  const T pi = T(3.14159265358979323846264338327950288);
+  // p / (gamma - 1) as p * (1 / (gamma - 1)) and sqrt(pi lambda) as
+  // sqrt(pi) sqrt(lambda): one division and one square root fewer per
+  // side, each a last-bit change
+  const T igm1 = T(1.0) / (gamma - T(1.0));
+  const T sqrt_pi = T(1.77245385090551602729816748334114518);
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
     const T sign = side == 0 ? T(-1.0) : T(1.0);
@@ -249,14 +255,15 @@ __device__ inline int kinetic_fluid_flux(const PrimT<T> st[2], T gamma,
     const T p = st[side].p;
     const T vx = st[side].vx, vy = st[side].vy, vz = st[side].vz;
     const T v2 = dot3(vx, vy, vz, vx, vy, vz);
-    const T energy = T(0.5) * rho * v2 + p / (gamma - T(1.0));
+    const T energy = T(0.5) * rho * v2 + p * igm1;
     const T lambda = rho / (T(2.0) * p);
+    const T sl = Num<T>::sqrt_(lambda);
     const T vn = dot3(fr.nx, fr.ny, fr.nz, vx, vy, vz);
     const T vt1 = dot3(fr.t1x, fr.t1y, fr.t1z, vx, vy, vz);
     const T vt2 = dot3(fr.t2x, fr.t2y, fr.t2z, vx, vy, vz);
-    const T zeroth = T(0.5) * Num<T>::erfc_(sign * Num<T>::sqrt_(lambda) * vn);
+    const T zeroth = T(0.5) * Num<T>::erfc_(sign * sl * vn);
     const T first = vn * zeroth - T(0.5) * sign * Num<T>::exp_(-lambda * vn * vn) /
-                                      Num<T>::sqrt_(pi * lambda);
+                                      (sqrt_pi * sl);
     fl->vn[side] = vn;
     fl->f[0] += rho * first;
     fl->f[4] += (energy + T(0.5) * p) * first + T(0.5) * p * zeroth * vn;
@@ -303,6 +310,7 @@ __device__ inline int kinetic_maxwell_flux(const PrimT<T> st[2], const T b[2][3]
   mx->alfven = T(0.0);
   mx->pmag = T(0.0);
   const T nrm[3] = {fr.nx, fr.ny, fr.nz};
+  const T ic2 = use_boris ? T(1.0) / (c * c) : T(0.0);
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
     const T sign = side == 0 ? T(-1.0) : T(1.0);
@@ -316,9 +324,11 @@ __device__ inline int kinetic_maxwell_flux(const PrimT<T> st[2], const T b[2][3]
       tz = b[side][2] + b0[2];
     }
     const T t2 = dot3(tx, ty, tz, tx, ty, tz);
-    const T va2 = t2 / st[side].rho;
-    const T cva2 = use_boris ? va2 / (T(1.0) + va2 / (c * c)) : va2;
-    const T lambda = T(1.0) / (T(2.0) * st[side].p / st[side].rho + cva2);
+    // 1 / rho and 1 / c^2 once: two divisions fewer per side
+    const T irho = T(1.0) / st[side].rho;
+    const T va2 = t2 * irho;
+    const T cva2 = use_boris ? va2 / (T(1.0) + va2 * ic2) : va2;
+    const T lambda = T(1.0) / (T(2.0) * st[side].p * irho + cva2);
     const T zeroth = T(0.5) * Num<T>::erfc_(sign * Num<T>::sqrt_(lambda) * vn[side]);
     mx->alfven += T(0.5) * Num<T>::sqrt_(cva2);
     mx->pmag += T(0.5) * t2;

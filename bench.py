@@ -781,7 +781,8 @@ def run_mi(lib, torch, device, solves):
 
     tensor_ms, tensor_its = tensor_times(0)
     colored_ms, colored_its = tensor_times(1)
-    two_level, learned = mi_flexible(lib, cs[0], solves)
+    pcg = pedersen_pcg_times(lib, torch, device, solves, flush)
+    two_level, learned = mi_flexible(lib, cs[0], solves, pcg)
     ms_one, it_one, csize = out["one"]
     ms_pair, it_pair, _ = out["pair"]
     us_iter = ms_one * 1e3 / it_one[0]
@@ -810,10 +811,72 @@ def run_mi(lib, torch, device, solves):
                                         "sweep": "four-colour SSOR, each colour by the whole cluster"}},
         "tensor_two_level": two_level,
         "tensor_learned": learned,
+        "pedersen_pcg": pcg,
     }
 
 
-def mi_flexible(lib, case, solves, train_steps=600):
+def pedersen_case(hemisphere):
+    """The C5 conductances with Hall = 0 and one conductance at the pole
+    point (the pole row's mean): the operator on which plain PCG is defined
+    (symmetric positive definite)."""
+    from gamera_cube_b200 import cases
+    npl, nt = MI_GRID
+    c = cases.mi_case(npl, nt, seed=MI_SEED, hemisphere=hemisphere)
+    ped = c.pedersen.copy()
+    ped[0, :] = ped[0, :].mean()
+    import numpy as np
+    return cases.MiCase(c.config, c.fac, np.ascontiguousarray(ped), np.zeros_like(ped),
+                        c.potential)
+
+
+def pedersen_pcg_times(lib, torch, device, solves, flush):
+    """Plain PCG (Jacobi) on the variable-Pedersen, Hall-free operator,
+    181 x 361, rel. residual 1e-8, zero guess: one hemisphere per launch and
+    both in one launch; device time with CUDA events, L2 flushed between
+    solves."""
+    import numpy as np
+    from gamera_cube_b200 import abi, cases
+    hs = [pedersen_case(h) for h in (cases.NORTH, cases.SOUTH)]
+    npl, nt = MI_GRID
+    out = {"operator": "variable Pedersen (C5 field, pole row its mean), Hall = 0: "
+                       "symmetric positive definite; Jacobi-preconditioned CG, "
+                       "one thread-block cluster per hemisphere"}
+    for label, count in (("one", 1), ("pair", 2)):
+        cfgs = (abi.MiSolverConfig * count)(*[c.config for c in hs[:count]])
+        ped = np.ascontiguousarray(np.concatenate([c.pedersen.ravel() for c in hs[:count]]))
+        plan = C.c_void_p()
+        if lib.gcs_mi_plan_create_pedersen(cfgs, ped.ctypes.data_as(C.POINTER(C.c_double)),
+                                           count, C.byref(plan)) != 0:
+            raise RuntimeError(lib.gcs_last_error().decode())
+        fac = torch.from_numpy(np.concatenate([c.fac.ravel() for c in hs[:count]])).to(device)
+        pot = torch.zeros_like(fac)
+        stats, status = (abi.MiSolverStats * count)(), (C.c_int * count)()
+        times = []
+        stream = torch.cuda.current_stream(device)
+        for q in range(3 + solves):
+            pot.zero_()
+            flush.fill_(float(q))
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            if lib.gcs_mi_solve_constant_pedersen_async(
+                    plan, C.c_void_p(fac.data_ptr()), C.c_void_p(pot.data_ptr()),
+                    C.c_void_p(stream.cuda_stream)) != 0:
+                raise RuntimeError(lib.gcs_last_error().decode())
+            ev1.record(stream)
+            if lib.gcs_mi_plan_results(plan, stats, status) != 0 or \
+                    any(status[h] != 0 for h in range(count)):
+                raise RuntimeError("Pedersen PCG did not converge")
+            if q >= 3:
+                times.append(ev0.elapsed_time(ev1))
+        lib.gcs_mi_plan_destroy(plan)
+        key = "ms_per_call" if count == 1 else "ms_per_call_both_hemispheres_one_launch"
+        out[key] = sorted(times)[len(times) // 2]
+        out["iterations" if count == 1 else "iterations_both"] = \
+            [stats[h].iterations for h in range(count)]
+    return out
+
+
+def mi_flexible(lib, case, solves, pcg=None, train_steps=600):
     """The conductance-tensor case by flexible GMRES: left two-level
     preconditioner (ring-mean coarse correction + damped Jacobi) alone, and
     with the learned network as the right preconditioner after a short
@@ -854,6 +917,31 @@ def mi_flexible(lib, case, solves, train_steps=600):
                             "loss_last": float(np.mean(losses[-20:]))},
                "ms_per_call": sec * 1e3, "iterations": st.iterations,
                "fell_back_to_reference_algorithm": bool(fb), "converged": rc == 0}
+    if pcg is not None:
+        # the same learned method and the two-level method on the operator
+        # where plain PCG is defined (Hall = 0), against plain PCG
+        from gamera_cube_b200 import cases as _cases
+        hcase = pedersen_case(_cases.NORTH)
+        hcase.config.maximum_iterations = 3000
+        net = learn.create_net(lib, hcase.config, batch=8, seed=3)
+        try:
+            pool = learn.Pool(lib, npl=hcase.config.longitude_count,
+                              nt=hcase.config.colatitude_count, random_fields=128, solved=4,
+                              conductances=8, hall_ratio=0.0)
+            learn.train(lib, net, pool, steps=train_steps, batch=8, lr=1e-3)
+            learn.solve(lib, net, hcase, method=0)
+            rc0, _, st0, fb0, sec0 = learn.solve(lib, net, hcase, method=0)
+        finally:
+            lib.gcs_mi_net_destroy(net)
+        rc2, _, st2, fb2, sec2 = learn.solve(lib, None, hcase, method=2)
+        learned["on_pcg_operator"] = {
+            "operator": pcg["operator"],
+            "learned_ms_per_call": sec0 * 1e3, "learned_iterations": st0.iterations,
+            "learned_fell_back": bool(fb0),
+            "two_level_ms_per_call": sec2 * 1e3, "two_level_iterations": st2.iterations,
+            "plain_pcg_ms_per_call": pcg["ms_per_call"],
+            "plain_pcg_iterations": pcg["iterations"][0],
+            "speedup_learned_over_plain_pcg": pcg["ms_per_call"] / (sec0 * 1e3)}
     return two_level, learned
 
 

@@ -155,6 +155,11 @@ def _load(path=None):
     sig.update(abi.ensemble_signatures())
     sig["gcs_context_set_mi_coupling"] = (C.c_int, [C.c_void_p, C.c_void_p, C.c_int])
     sig["gcs_context_time"] = (C.c_int, [C.c_void_p, P(C.c_double)])
+    sig["gcs_mi_plan_create_pedersen"] = (C.c_int, [P(abi.MiSolverConfig), P(C.c_double),
+                                                    C.c_int, P(C.c_void_p)])
+    sig["gcs_mi_solve_pedersen_pcg"] = (C.c_int, [P(abi.MiSolverConfig), P(C.c_double),
+                                                  P(C.c_double), P(C.c_double),
+                                                  P(abi.MiSolverStats)])
     sig["gcs_context_mi_dipole_create"] = (
         C.c_int, [C.c_void_p, P(abi.EarthStartup), P(abi.MiDipoleConfig),
                   P(C.c_void_p)])

@@ -69,6 +69,15 @@ struct System {
   int max_iter;
   int pad;
   const int *gate;  // when set, the solve runs only where *gate != 0
+  // Variable Pedersen conductance (Hall = 0) when coef is set (k_pcg only):
+  // the five-point stencil of the conductance-tensor operator
+  // (nonorthogonal_mi.c:776-865) per reduced unknown -- diagonal, lower,
+  // upper, longitude lower, longitude upper, `unknowns` entries each -- the
+  // pole edge coefficients and the pole diagonal; Jacobi on that diagonal.
+  const double *coef;
+  const double *pedge;
+  double diag0;
+  long long unknowns;
   double pe;        // pole edge coefficient (nonorthogonal_mi.c:324-334)
   double neg_r2;    // -R^2
   double low;       // low-latitude Dirichlet potential
@@ -161,6 +170,24 @@ __device__ __forceinline__ double apply_row(const double *s, const Band &b,
                  rw.lon * (2.0 * c - sm - sp));
 }
 
+// Tensor-stencil row (nonorthogonal_mi.c:872-897, Hall = 0), evaluated in
+// the reference's order; ci is the reduced index of the point.
+__device__ __forceinline__ double apply_var(const double *s, const Band &b,
+                                            const System &S, int np, int l, int j,
+                                            int p, double pole, long long ci) {
+  const long long n = S.unknowns;
+  const double c = s[p];
+  const double sm = j == 0 ? s[p + np - 1] : s[p - 1];
+  const double sp = j == np - 1 ? s[p - np + 1] : s[p + 1];
+  double lv, uv;
+  if (l > 0) lv = s[p - np];
+  else lv = b.top ? pole : b.hs_up[j];
+  if (l < b.nrow - 1) uv = s[p + np];
+  else uv = b.bottom ? 0.0 : b.hs_dn[j];
+  return S.coef[ci] * c + S.coef[n + ci] * lv + S.coef[2 * n + ci] * uv +
+         S.coef[3 * n + ci] * sm + S.coef[4 * n + ci] * sp;
+}
+
 // Sets s[p] of an owned point and pushes it to the neighbour whose halo
 // row holds it.
 __device__ __forceinline__ void set_s(double *s, const Band &b, int l, int j, int p,
@@ -227,6 +254,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const bool lead = b.top;
   const double dnp = (double)np;
   const double ps = dnp * S.pe;  // pole diagonal and pole residual scale
+  const bool var = S.coef != nullptr;
+  const double pd = var ? S.diag0 : ps;  // pole diagonal of the Jacobi step
   const Walk W(t, np);
   int ctr = 0;
 
@@ -260,23 +289,25 @@ __global__ void __launch_bounds__(kThreads, 1)
       const Row &rw = rt[l];
       const double f = S.fac[(size_t)(b.ra + l + 1) * np + j];
       const double u = S.neg_r2 * f * rw.inc;
-      const double rhs = rw.w * u + rw.extra;
-      const double ax = apply_row(s, b, rw, np, l, j, p, pole);
+      const double rhs = rw.w * u + (var ? 0.0 : rw.extra);
+      const long long ci = 1 + (long long)(b.ra + l) * np + j;
+      const double ax = var ? apply_var(s, b, S, np, l, j, p, pole, ci)
+                            : apply_row(s, b, rw, np, l, j, p, pole);
       const double r = rhs - ax;
       rs[p] = r;
       const double q = r * rw.rw;
       v[0] += q * q;
       v[1] += u * u;
       v[2] += isfinite(f) ? 0.0 : 1.0;
-      if (b.ra + l == 0) v[3] += s[p];
+      if (b.ra + l == 0) v[3] += var ? S.pedge[j] * s[p] : s[p];
     }
     block_sum<4>(v, wbuf);
     if (lead) {
-      const double ax0 = S.pe * (dnp * pole - v[3]);
+      const double ax0 = var ? S.diag0 * pole - v[3] : S.pe * (dnp * pole - v[3]);
       r0 = 0.0 - ax0;
       const double pr = r0 / ps;
       v[0] += dnp * pr * pr;
-      v[1] += dnp * S.low * S.low;
+      if (!var) v[1] += dnp * S.low * S.low;
     }
     out[0] = v[0];
     out[1] = v[1];
@@ -289,13 +320,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     double v[1] = {0.0};
     GCS_MI_FOR_POINTS(W, P, np) {
       const double r = rs[p];
-      const double z = r * rt[l].rdg;
+      const double z = var ? r / S.coef[1 + (long long)(b.ra + l) * np + j]
+                           : r * rt[l].rdg;
       set_s(s, b, l, j, p, z);
       v[0] += r * z;
     }
     block_sum<1>(v, wbuf);
     if (lead) {
-      const double z0 = r0 / ps;
+      const double z0 = r0 / pd;
       v[0] += r0 * z0;
       if (t == 0) pole_s = z0;
     }
@@ -322,16 +354,18 @@ __global__ void __launch_bounds__(kThreads, 1)
       double v[2] = {0.0, 0.0};  // s.As, first-ring sum of s
       const double pole = lead ? pole_s : 0.0;
       GCS_MI_FOR_POINTS(W, P, np) {
-        const double a = apply_row(s, b, rt[l], np, l, j, p, pole);
+        const double a = var ? apply_var(s, b, S, np, l, j, p, pole,
+                                         1 + (long long)(b.ra + l) * np + j)
+                             : apply_row(s, b, rt[l], np, l, j, p, pole);
         as[p] = a;
         v[0] += s[p] * a;
-        if (b.ra + l == 0) v[1] += s[p];
+        if (b.ra + l == 0) v[1] += var ? S.pedge[j] * s[p] : s[p];
       }
       block_sum<2>(v, wbuf);
       double As0 = 0.0;
       double den[1] = {v[0]};
       if (lead) {
-        As0 = S.pe * (dnp * pole - v[1]);
+        As0 = var ? S.diag0 * pole - v[1] : S.pe * (dnp * pole - v[1]);
         den[0] += pole * As0;
       }
       cluster_sum<1>(cl, den, slots, ctr, rank, csize);
@@ -347,7 +381,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const double r = rs[p] - alpha * as[p];
         rs[p] = r;
         const double q = r * rw.rw;
-        const double z = r * rw.rdg;
+        const double z = var ? r / S.coef[1 + (long long)(b.ra + l) * np + j] : r * rw.rdg;
         w2[0] += q * q;
         w2[1] += r * z;
         if (l == 0 && !b.top) b.peer_up_hz[j] = z;
@@ -359,7 +393,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         r0 -= alpha * As0;
         const double pr = r0 / ps;
         w2[0] += dnp * pr * pr;
-        w2[1] += r0 * (r0 / ps);
+        w2[1] += r0 * (r0 / pd);
       }
       cluster_sum<2>(cl, w2, slots, ctr, rank, csize);
       final_res = sqrt(fmax(0.0, w2[0]));
@@ -381,12 +415,18 @@ __global__ void __launch_bounds__(kThreads, 1)
       const double rho_new = w2[1];
       if (!isfinite(rho_new) || rho_new <= DBL_MIN) break;
       const double beta = rho_new / rho;
-      GCS_MI_FOR_POINTS(W, P, np) { s[p] = rs[p] * rt[l].rdg + beta * s[p]; }
+      if (var) {
+        GCS_MI_FOR_POINTS(W, P, np) {
+          s[p] = rs[p] / S.coef[1 + (long long)(b.ra + l) * np + j] + beta * s[p];
+        }
+      } else {
+        GCS_MI_FOR_POINTS(W, P, np) { s[p] = rs[p] * rt[l].rdg + beta * s[p]; }
+      }
       for (int j = t; j < np; j += kThreads) {
         if (!b.top) b.hs_up[j] = b.hz_up[j] + beta * b.hs_up[j];
         if (!b.bottom) b.hs_dn[j] = b.hz_dn[j] + beta * b.hs_dn[j];
       }
-      if (lead && t == 0) pole_s = r0 / ps + beta * pole;
+      if (lead && t == 0) pole_s = r0 / pd + beta * pole;
       rho = rho_new;
       __syncthreads();
     }
@@ -947,6 +987,7 @@ struct gcs_mi_plan {
   double *d_pot = nullptr;        // count * nt * np
   gamera_mi_solver_stats *d_stats = nullptr;
   int *d_status = nullptr;
+  double *d_coef = nullptr;       // variable Pedersen: count * (5 unknowns + np)
   std::vector<System> host_sys;
   cudaStream_t stream = nullptr;  // stream of the last solve
 };
@@ -963,6 +1004,7 @@ void plan_free(gcs_mi_plan *p) {
   cudaFree(p->d_pot);
   cudaFree(p->d_stats);
   cudaFree(p->d_status);
+  cudaFree(p->d_coef);
   delete p;
 }
 
@@ -980,10 +1022,12 @@ bool cuda_ok(cudaError_t e, const char *what) {
 // most 16) whose rows fit its registers; otherwise the shared-memory kernel
 // with about 2048 unknowns per CTA (8 CTAs at most where the device cannot
 // co-schedule 16).
-int choose_shape(gcs_mi_plan *p) {
+int choose_shape(gcs_mi_plan *p, bool variable = false) {
   const int R = p->nt - 2, np = p->np;
   const int threads = (np + 31) / 32 * 32;
+  // the variable-conductance mode lives in the shared-memory kernel
   for (int mr : {4, 8, 12, 16}) {
+    if (variable) break;
     Shape sh;
     sh.kernel = col_kernel(mr);
     sh.csize = (R + mr - 1) / mr;
@@ -1020,7 +1064,56 @@ int choose_shape(gcs_mi_plan *p) {
   return -1;
 }
 
-gcs_mi_plan *plan_create(const gamera_mi_solver_config *configs, int count) {
+// The five-point stencil of the conductance-tensor operator with Hall = 0
+// (nonorthogonal_mi.c:744-865, same operations): per reduced unknown the
+// diagonal, lower, upper, longitude-lower and longitude-upper coefficients
+// (`unknowns` entries each), then the np pole edge coefficients; returns the
+// pole diagonal.
+double build_pedersen_stencil(const gamera_mi_solver_config *c, const double *ped,
+                              double *coef) {
+  const size_t np = c->longitude_count, nt = c->colatitude_count;
+  const size_t n = 1U + np * (nt - 2U);
+  const double dth = c->maximum_colatitude / (double)(nt - 1U);
+  const double dph = 2.0 * acos(-1.0) / (double)np;
+  auto incsq = [](double th) {
+    const double co = cos(th);
+    return 4.0 * co * co / (1.0 + 3.0 * co * co);
+  };
+  auto P = [&](size_t i, size_t j) { return ped[i * np + j]; };
+  double *pedge = coef + 5 * n;
+  double mean = 0.0;
+  for (size_t j = 0; j < np; ++j) mean += P(0, j) / (double)np;
+  const double half = 0.5 * dth;
+  double diag0 = 0.0;
+  for (size_t j = 0; j < np; ++j) {
+    const double face = 0.5 * (mean + P(1, j));
+    pedge[j] = sin(half) * face / (incsq(half) * dth * dth);
+    diag0 += pedge[j];
+  }
+  coef[0] = diag0;
+  for (int q = 1; q < 5; ++q) coef[q * n] = 0.0;
+  for (size_t i = 1; i + 1 < nt; ++i) {
+    const double th = (double)i * dth, sine = sin(th);
+    const double lth = th - 0.5 * dth, uth = th + 0.5 * dth;
+    for (size_t j = 0; j < np; ++j) {
+      const size_t jm = j == 0 ? np - 1 : j - 1, jp = j + 1 == np ? 0 : j + 1;
+      const double lower = sin(lth) * 0.5 * (P(i, j) + P(i - 1, j)) / (incsq(lth) * dth * dth);
+      const double upper = sin(uth) * 0.5 * (P(i, j) + P(i + 1, j)) / (incsq(uth) * dth * dth);
+      const double ll = 0.5 * (P(i, j) + P(i, jm)) / (sine * dph * dph);
+      const double lu = 0.5 * (P(i, j) + P(i, jp)) / (sine * dph * dph);
+      const size_t ci = 1 + (i - 1) * np + j;
+      coef[ci] = lower + upper + ll + lu;
+      coef[n + ci] = -lower;
+      coef[2 * n + ci] = -upper;
+      coef[3 * n + ci] = -ll;
+      coef[4 * n + ci] = -lu;
+    }
+  }
+  return diag0;
+}
+
+gcs_mi_plan *plan_create(const gamera_mi_solver_config *configs, int count,
+                         const double *pedersen = nullptr) {
   if (count < 1) {
     set_api_error("MI plan needs at least one system");
     return nullptr;
@@ -1045,7 +1138,7 @@ gcs_mi_plan *plan_create(const gamera_mi_solver_config *configs, int count) {
   p->np = (int)configs[0].longitude_count;
   p->nt = (int)configs[0].colatitude_count;
   p->configs.assign(configs, configs + count);
-  if (choose_shape(p) != 0) {
+  if (choose_shape(p, pedersen != nullptr) != 0) {
     plan_free(p);
     return nullptr;
   }
@@ -1076,6 +1169,28 @@ gcs_mi_plan *plan_create(const gamera_mi_solver_config *configs, int count) {
     S.max_iter = c->maximum_iterations;
     S.pad = 0;
     S.gate = nullptr;
+    S.coef = nullptr;
+    S.pedge = nullptr;
+    S.diag0 = 0.0;
+    S.unknowns = (long long)(1 + (size_t)p->np * R);
+    if (pedersen) {
+      // variable Pedersen conductance of system s (nt * np per system)
+      const size_t n = 1 + (size_t)p->np * R, per = 5 * n + p->np;
+      if (!p->d_coef &&
+          !cuda_ok(cudaMalloc(&p->d_coef, count * per * sizeof(double)), "cudaMalloc")) {
+        plan_free(p);
+        return nullptr;
+      }
+      std::vector<double> coef(per);
+      S.diag0 = build_pedersen_stencil(c, pedersen + s * nodes, coef.data());
+      if (!cuda_ok(cudaMemcpy(p->d_coef + s * per, coef.data(), per * sizeof(double),
+                              cudaMemcpyHostToDevice), "cudaMemcpy")) {
+        plan_free(p);
+        return nullptr;
+      }
+      S.coef = p->d_coef + s * per;
+      S.pedge = S.coef + 5 * n;
+    }
     S.pe = pole_edge(c);
     S.neg_r2 = -(c->ionosphere_radius_m * c->ionosphere_radius_m);
     S.low = c->low_latitude_potential_v;
@@ -1234,6 +1349,66 @@ int gcs_mi_plan_results(gcs_mi_plan *plan, gamera_mi_solver_stats *stats, int *s
 }
 
 // Drop-in for nonorthogonal_mi.c:433 (host arrays, synchronous).
+int gcs_mi_plan_create_pedersen(const gamera_mi_solver_config *configs,
+                                const double *pedersen, int count, gcs_mi_plan **plan) {
+  if (!configs || !pedersen || !plan || count < 1) {
+    set_api_error("null argument");
+    return -1;
+  }
+  *plan = nullptr;
+  for (int s = 0; s < count; ++s)
+    if (!valid_config(&configs[s])) {
+      set_api_error("invalid MI solver configuration");
+      return -1;
+    }
+  const size_t nodes = configs[0].longitude_count * configs[0].colatitude_count;
+  for (size_t q = 0; q < (size_t)count * nodes; ++q)
+    if (!std::isfinite(pedersen[q]) || pedersen[q] <= 0.0) {
+      set_api_error("Pedersen conductance must be finite and positive");
+      return -1;
+    }
+  *plan = plan_create(configs, count, pedersen);
+  return *plan ? 0 : -1;
+}
+
+int gcs_mi_solve_pedersen_pcg(const gamera_mi_solver_config *config, const double *fac_a_m2,
+                              const double *pedersen, double *potential_v,
+                              gamera_mi_solver_stats *stats) {
+  if (!valid_config(config) || fac_a_m2 == nullptr || pedersen == nullptr ||
+      potential_v == nullptr) {
+    set_api_error("invalid MI solver arguments");
+    return -1;
+  }
+  gcs_mi_plan *p = nullptr;
+  if (gcs_mi_plan_create_pedersen(config, pedersen, 1, &p) != 0) return -1;
+  const size_t bytes = config->longitude_count * config->colatitude_count * sizeof(double);
+  cudaStream_t st = nullptr;
+  int status = 2;
+  gamera_mi_solver_stats s = {};
+  const bool ok =
+      cuda_ok(cudaMemcpyAsync(p->d_fac, fac_a_m2, bytes, cudaMemcpyHostToDevice, st),
+              "cudaMemcpyAsync") &&
+      cuda_ok(cudaMemcpyAsync(p->d_pot, potential_v, bytes, cudaMemcpyHostToDevice, st),
+              "cudaMemcpyAsync") &&
+      plan_launch(p, st) == 0 &&
+      cuda_ok(cudaMemcpyAsync(potential_v, p->d_pot, bytes, cudaMemcpyDeviceToHost, st),
+              "cudaMemcpyAsync") &&
+      cuda_ok(cudaMemcpyAsync(&s, p->d_stats, sizeof(s), cudaMemcpyDeviceToHost, st),
+              "cudaMemcpyAsync") &&
+      cuda_ok(cudaMemcpyAsync(&status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                              st),
+              "cudaMemcpyAsync") &&
+      cuda_ok(cudaStreamSynchronize(st), "MI solve");
+  plan_free(p);
+  if (!ok) return -1;
+  if (status == 2) {
+    set_api_error("non-finite field-aligned current");
+    return -1;
+  }
+  if (stats) *stats = s;
+  return status == 0 ? 0 : -1;
+}
+
 int gamera_mi_solve_constant_pedersen(const gamera_mi_solver_config *config,
                                       const double *fac_a_m2, double *potential_v,
                                       gamera_mi_solver_stats *stats) {

@@ -141,11 +141,11 @@ class Pool:
     targets [R][np] (unit RMS)."""
 
     def __init__(self, lib, npl=361, nt=181, max_colatitude_deg=45.0, random_fields=384,
-                 solved=16, conductances=16, seed=1234):
+                 solved=16, conductances=16, seed=1234, hall_ratio=1.5):
         rng = np.random.default_rng(seed)
         self.npl, self.nt = npl, nt
         inputs, targets = [], []
-        cond = [cases.mi_case(npl, nt, seed=seed + 17 * c,
+        cond = [cases.mi_case(npl, nt, seed=seed + 17 * c, hall_ratio=hall_ratio,
                               max_colatitude_deg=max_colatitude_deg) for c in range(conductances)]
         self.triples = 0
         ops = {}
@@ -159,7 +159,7 @@ class Pool:
             self._add(inputs, targets, A, E, T, A @ reduce(e), reduce(e),
                       features(cfg, case.pedersen, case.hall))
         for k in range(solved):
-            case = cases.mi_case(npl, nt, seed=seed + 1000 + k,
+            case = cases.mi_case(npl, nt, seed=seed + 1000 + k, hall_ratio=hall_ratio,
                                  max_colatitude_deg=max_colatitude_deg, max_iterations=20000)
             pot = case.potential.copy()
             st = abi.MiSolverStats()

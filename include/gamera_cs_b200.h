@@ -693,6 +693,23 @@ int gcs_context_mi_dipole_create(gcs_context *ctx, const gamera_cs_earth_startup
 int gcs_context_set_mi_coupling(gcs_context *ctx, gamera_cs_mi_dipole *mi, int every_steps);
 int gcs_mi_plan_create(const gamera_mi_solver_config *configs, int count,
                        gcs_mi_plan **plan);
+/* Plain PCG on the variable-Pedersen, Hall-free operator.  No reference
+ * counterpart: the reference solves the conductance tensor by SSOR-BiCGStab
+ * (gamera_mi_solve_conductance_tensor); with Hall = 0 and a single pole
+ * conductance (pedersen row 0 uniform) that operator is symmetric positive
+ * definite, and this is Jacobi-preconditioned CG on it: the five-point
+ * stencil of nonorthogonal_mi.c:744-865 with Hall = 0, the reference
+ * tensor solve's right-hand side and residual norm
+ * (nonorthogonal_mi.c:1000-1044, :415-431), true-residual check at
+ * convergence and every 1024 iterations.  pedersen: count * nt * np values
+ * (row 0 = pole).  The plan solves through gcs_mi_solve_constant_pedersen_async
+ * and reports through gcs_mi_plan_results like a constant-Pedersen plan. */
+int gcs_mi_plan_create_pedersen(const gamera_mi_solver_config *configs,
+                                const double *pedersen, int count, gcs_mi_plan **plan);
+/* The same solve on host arrays, synchronous (0 converged, -1 otherwise). */
+int gcs_mi_solve_pedersen_pcg(const gamera_mi_solver_config *config, const double *fac_a_m2,
+                              const double *pedersen, double *potential_v,
+                              gamera_mi_solver_stats *stats);
 void gcs_mi_plan_destroy(gcs_mi_plan *plan);
 int gcs_mi_plan_info(const gcs_mi_plan *plan, int *cluster_ctas,
                      int *threads_per_cta, size_t *shared_bytes);

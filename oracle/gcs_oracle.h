@@ -88,6 +88,9 @@ int gcso_mi_apply_conductance_tensor(const gamera_mi_solver_config *config,
                                      const double *pedersen,
                                      const double *hall,
                                      const double *potential, double *result);
+int gcso_mi_solve_pedersen_pcg(const gamera_mi_solver_config *config, const double *fac,
+                               const double *pedersen, double *potential,
+                               gamera_mi_solver_stats *stats);
 int gcso_mi_solve_conductance_tensor(const gamera_mi_solver_config *config,
                                      const double *fac, const double *pedersen,
                                      const double *hall, double *potential,

@@ -76,6 +76,9 @@ def lib():
                 ("gcso_mi_apply_conductance_tensor", C.c_int,
                  [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double),
                   P(C.c_double), P(C.c_double)]),
+                ("gcso_mi_solve_pedersen_pcg", C.c_int,
+                 [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double), P(C.c_double),
+                  P(abi.MiSolverStats)]),
                 ("gcso_mi_solve_conductance_tensor", C.c_int,
                  [P(abi.MiSolverConfig), P(C.c_double), P(C.c_double),
                   P(C.c_double), P(C.c_double), P(abi.MiSolverStats)])]:

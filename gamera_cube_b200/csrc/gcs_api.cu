@@ -290,16 +290,12 @@ int run_step(gcs_context *ctx, const gcs::Opts &O, int driver_mode,
     gcs::launch_edge_sync(X, s);
     mk.mark(kSlotEdgeSync);
   }
-  // the update stores the final B (and, with the driver's CFL step, the
-  // CFL candidates) of the cells without seam faces; the final recovery
-  // does the rest
-  const bool cfl = driver_mode && !post_control;
-  gcs::launch_update(X, O, O.u_mhd ? (1 | (cfl ? 2 : 0)) : 0, s);
+  gcs::launch_update(X, O, s);
   mk.mark(kSlotUpdate);
   if (O.u_mhd) {
     gcs::launch_seam_sync(X, 1, s);
     mk.mark(kSlotSeamPhiFinal);
-    gcs::launch_recover(X, O, cfl, 1, s);
+    gcs::launch_recover(X, O, driver_mode && !post_control, s);
     mk.mark(kSlotRecover);
   }
   if (post_control) {

@@ -239,10 +239,7 @@ __global__ void __launch_bounds__(256) k_recover(Dims D, DevState S, DevGeom G,
     const long long c = f * D.Nn + D.node(i, j, k);
     double bn[3];
     bool ok = true;
-    if ((mode & 4) && interior_cell(D, i, j, k)) {
-      // final B and CFL candidate of this cell came from the cell update
-      ok = false;
-    } else if (mode & 1) {
+    if (mode & 1) {
       double phi[6];
       const long long sdir[3] = {D.stride(0), D.stride(1), 1};
 #pragma unroll
@@ -466,7 +463,7 @@ void launch_edge_sync(const Ctx &X, cudaStream_t s) {
         X.D, X.edge_offsets, X.edge_members, X.n_edge_groups, X.S, X.status);
 }
 
-void launch_update(const Ctx &X, const Opts &O, int fuse, cudaStream_t s) {
+void launch_update(const Ctx &X, const Opts &O, cudaStream_t s) {
   const Dims &D = X.D;
   const Tile t = X.tile[kTileCt], tu = X.tile[kTileUpdate];
   k_ct<0><<<tile_grid(D.E0 + 1, D.E1, D.E2, t), tile_block(t), 0, s>>>(
@@ -476,15 +473,15 @@ void launch_update(const Ctx &X, const Opts &O, int fuse, cudaStream_t s) {
   k_ct<2><<<tile_grid(D.E0, D.E1, D.E2 + 1, t), tile_block(t), 0, s>>>(
       D, X.S, O, X.params, X.status);
   k_update<<<tile_grid(D.E0, D.E1, D.E2, tu), tile_block(tu), 0, s>>>(
-      D, X.S, X.G, X.BG, O, X.params, X.status, fuse);
+      D, X.S, X.G, X.BG, O, X.params, X.status);
 }
 
-void launch_recover(const Ctx &X, const Opts &O, int with_cfl, int after_fused,
+void launch_recover(const Ctx &X, const Opts &O, int with_cfl,
                     cudaStream_t s) {
   const Dims &D = X.D;
   const Tile t = X.tile[kTileRecover];
   k_recover<<<tile_grid(D.E0, D.E1, D.E2, t), tile_block(t), 0, s>>>(
-      D, X.S, X.G, X.BG, O, 1 | (with_cfl ? 2 : 0) | (after_fused ? 4 : 0), X.status);
+      D, X.S, X.G, X.BG, O, 1 | (with_cfl ? 2 : 0), X.status);
 }
 
 void launch_timestep(const Ctx &X, const Opts &O, cudaStream_t s) {
@@ -522,9 +519,9 @@ void launch_step(const Ctx &X, const Opts &O, int driver_mode,
     launch_emf(X, O, s);
     launch_edge_sync(X, s);
   }
-  launch_update(X, O, O.u_mhd ? (1 | (driver_mode ? 2 : 0)) : 0, s);
+  launch_update(X, O, s);
   if (O.u_mhd) launch_seam_sync(X, 1, s);
-  if (O.u_mhd) launch_recover(X, O, driver_mode, 1, s);
+  if (O.u_mhd) launch_recover(X, O, driver_mode, s);
   if (driver_mode) {
     launch_count_step(X, s);
     launch_next_dt(X, O.dt_fraction, s);

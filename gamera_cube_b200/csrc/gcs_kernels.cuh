@@ -84,11 +84,8 @@ void launch_emf(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_face_velocities(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_edge_emfs(const Ctx &X, const Opts &O, cudaStream_t s);
 void launch_edge_sync(const Ctx &X, cudaStream_t s);
-// fuse: 1 the update also stores the final B of interior cells (no seam
-// face), 2 and their CFL candidates; the final recovery then runs with
-// after_fused set and skips those cells.
-void launch_update(const Ctx &X, const Opts &O, int fuse, cudaStream_t s);
-void launch_recover(const Ctx &X, const Opts &O, int with_cfl, int after_fused,
+void launch_update(const Ctx &X, const Opts &O, cudaStream_t s);
+void launch_recover(const Ctx &X, const Opts &O, int with_cfl,
                     cudaStream_t s);
 void launch_next_dt(const Ctx &X, double fraction, cudaStream_t s);
 void launch_count_step(const Ctx &X, cudaStream_t s);

@@ -450,160 +450,85 @@ __global__ void k_ct(Dims D, DevState S, Opts O, const StepParams *prm, DevStatu
 // nonorthogonal_sweep.c:550-622): save U, B as old on every cell, then on
 // active cells U += dt * rate, recover B from the CT-updated Phi, and apply
 // the Boris (nonorthogonal_state.c:161-280) or Maxwell momentum update.
-//
-// fuse & 1: an interior active cell (none of its faces on a cube seam) also
-// stores that recovered B as its final cell B: the final seam sync changes
-// only seam faces, so the step's final recovery (k_recover) would compute
-// the same value, and skips these cells.  fuse & 2: those cells' CFL step
-// candidates (nonorthogonal_step.c:479-516, the arithmetic of k_recover)
-// enter the step's minimum here.
-__device__ inline bool interior_cell(const Dims &D, int i, int j, int k) {
-  return i >= D.g && i < D.g + D.nr && j > D.g && j < D.g + D.n - 1 && k > D.g &&
-         k < D.g + D.n - 1;
-}
-
-// CFL candidate of a cell with primitives from u and total field bn (+ B0).
-__device__ inline bool cfl_candidate(const double u[5], const double bn[3], long long c,
-                                     const DevGeom &G, const DevBg &BG, const Opts &O,
-                                     double *cand) {
-  Prim p;
-  if (cons_to_prim(u, O.t_gamma, O.t_rho_floor, O.t_p_floor, &p)) return false;
-  const double cs = sqrt(O.t_gamma * p.p / p.rho);
-  double va = 0.0;
-  if (O.t_mhd) {
-    double bx = bn[0], by = bn[1], bz = bn[2];
-    if (O.t_bg) {
-      bx = bn[0] + BG.b0[0][c];
-      by = bn[1] + BG.b0[1][c];
-      bz = bn[2] + BG.b0[2][c];
-    }
-    double s2 = 0.0;
-    s2 += bx * bx;
-    s2 += by * by;
-    s2 += bz * bz;
-    va = sqrt(s2) / sqrt(p.rho);
-    if (O.t_boris) va = O.t_c * va / hypot(O.t_c, va);
-  }
-  double v2 = 0.0;
-  v2 += p.vx * p.vx;
-  v2 += p.vy * p.vy;
-  v2 += p.vz * p.vz;
-  const double speed = sqrt(v2) + hypot(cs, va);
-  const double cand0 = O.t_cfl * G.cflmin[c] / speed;
-  if (!isfinite(cand0) || cand0 <= 0.0) return false;
-  *cand = cand0;
-  return true;
-}
-
 __global__ void __launch_bounds__(128, 6) k_update(Dims D, DevState S, DevGeom G,
                                                 DevBg BG, Opts O,
                                                 const StepParams *prm,
-                                                DevStatus *st, int fuse) {
-  // No early return: with fuse & 2 every thread reaches the block reduction.
-  const bool skip = failed(st);
-  double cand = DBL_MAX;
+                                                DevStatus *st) {
+  if (failed(st)) return;
   int f, i, j, k;
   const Box b{0, 0, 0, D.E1, D.E2, D.E0};
-  if (!skip && box_coord(b, &f, &i, &j, &k)) {
-    const long long c = f * D.Nn + D.node(i, j, k);
-    double u[5], bo[3];
+  if (!box_coord(b, &f, &i, &j, &k)) return;
+  const long long c = f * D.Nn + D.node(i, j, k);
+  double u[5], bo[3];
 #pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      u[m] = S.U[m][c];
-      S.Uo[m][c] = u[m];
-    }
+  for (int m = 0; m < 5; ++m) {
+    u[m] = S.U[m][c];
+    S.Uo[m][c] = u[m];
+  }
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    bo[m] = S.B[m][c];
+    S.Bo[m][c] = bo[m];
+  }
+  if (i < D.g || i >= D.g + D.nr || j < D.g || j >= D.g + D.n || k < D.g ||
+      k >= D.g + D.n)
+    return;
+  const double dt = prm->dt;
+  const double iv = G.ivol[c];
+  double rate[5], mrate[3];
+  const long long sdir[3] = {D.stride(0), D.stride(1), 1};
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    double diff = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) diff += S.F[d][m][c] - S.F[d][m][c + sdir[d]];
+    rate[m] = diff * iv;
+  }
+  const double uold[5] = {u[0], u[1], u[2], u[3], u[4]};
+#pragma unroll
+  for (int m = 0; m < 5; ++m) u[m] += dt * rate[m];
+  if (O.u_mhd) {
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      bo[m] = S.B[m][c];
-      S.Bo[m][c] = bo[m];
+      double diff = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        diff += S.M[d][m][c] - S.M[d][m][c + sdir[d]];
+      mrate[m] = diff * iv;
+      if (O.u_bg) mrate[m] += BG.force[m][c];
     }
-    if (i >= D.g && i < D.g + D.nr && j >= D.g && j < D.g + D.n && k >= D.g &&
-        k < D.g + D.n) {
-      const double dt = prm->dt;
-      const double iv = G.ivol[c];
-      double rate[5], mrate[3];
-      const long long sdir[3] = {D.stride(0), D.stride(1), 1};
+    double phi[6], bn[3];
 #pragma unroll
-      for (int m = 0; m < 5; ++m) {
-        double diff = 0.0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) diff += S.F[d][m][c] - S.F[d][m][c + sdir[d]];
-        rate[m] = diff * iv;
-      }
-      const double uold[5] = {u[0], u[1], u[2], u[3], u[4]};
-#pragma unroll
-      for (int m = 0; m < 5; ++m) u[m] += dt * rate[m];
-      bool ok = true;
-      double bn[3] = {0.0, 0.0, 0.0};
-      if (O.u_mhd) {
+    for (int d = 0; d < 3; ++d) {
+      phi[2 * d] = S.P[d][c];
+      phi[2 * d + 1] = S.P[d][c + sdir[d]];
+    }
+    if (!recover_cell(G, c, phi, bn)) {
+      fail(st, kStageRecoverUpdate, 0, f, i, j, k);
+      return;
+    }
+    if (O.u_boris) {
+      double nb[3] = {bn[0], bn[1], bn[2]};
+      double ob[3] = {bo[0], bo[1], bo[2]};
+      if (O.u_bg) {
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          double diff = 0.0;
-#pragma unroll
-          for (int d = 0; d < 3; ++d)
-            diff += S.M[d][m][c] - S.M[d][m][c + sdir[d]];
-          mrate[m] = diff * iv;
-          if (O.u_bg) mrate[m] += BG.force[m][c];
-        }
-        double phi[6];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          phi[2 * d] = S.P[d][c];
-          phi[2 * d + 1] = S.P[d][c + sdir[d]];
-        }
-        if (!recover_cell(G, c, phi, bn)) {
-          fail(st, kStageRecoverUpdate, 0, f, i, j, k);
-          ok = false;
-        } else if (O.u_boris) {
-          double nb[3] = {bn[0], bn[1], bn[2]};
-          double ob[3] = {bo[0], bo[1], bo[2]};
-          if (O.u_bg) {
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-              const double b0 = BG.b0[m][c];
-              nb[m] = bn[m] + b0;
-              ob[m] = bo[m] + b0;
-            }
-          }
-          if (apply_boris(u, uold, nb, ob, rate, mrate, O.u_c, dt, O.u_gamma,
-                          O.u_rho_floor, O.u_p_floor)) {
-            fail(st, kStageUpdate, 0, f, i, j, k);
-            ok = false;
-          }
-        } else {
-          apply_maxwell(u, mrate, dt, O.u_gamma, O.u_rho_floor, O.u_p_floor);
+          const double b0 = BG.b0[m][c];
+          nb[m] = bn[m] + b0;
+          ob[m] = bo[m] + b0;
         }
       }
-      if (ok) {
-#pragma unroll
-        for (int m = 0; m < 5; ++m) S.U[m][c] = u[m];
-        if ((fuse & 1) && O.u_mhd && interior_cell(D, i, j, k)) {
-#pragma unroll
-          for (int m = 0; m < 3; ++m) S.B[m][c] = bn[m];
-          if ((fuse & 2) && !cfl_candidate(u, bn, c, G, BG, O, &cand))
-            fail(st, kStageTimestep, 0, f, i, j, k);
-        }
+      if (apply_boris(u, uold, nb, ob, rate, mrate, O.u_c, dt, O.u_gamma,
+                      O.u_rho_floor, O.u_p_floor)) {
+        fail(st, kStageUpdate, 0, f, i, j, k);
+        return;
       }
+    } else {
+      apply_maxwell(u, mrate, dt, O.u_gamma, O.u_rho_floor, O.u_p_floor);
     }
   }
-  if (!(fuse & 2)) return;
-  // block min (positive doubles order as unsigned 64-bit integers)
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-    cand = fmin(cand, __shfl_down_sync(0xffffffffu, cand, o));
-  __shared__ double wmin[8];
-  const int lt = threadIdx.y * blockDim.x + threadIdx.x;
-  const int lane = lt & 31, warp = lt >> 5;
-  if (lane == 0) wmin[warp] = cand;
-  __syncthreads();
-  if (warp == 0) {
-    cand = lane < (int)((blockDim.x * blockDim.y) >> 5) ? wmin[lane] : DBL_MAX;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-      cand = fmin(cand, __shfl_down_sync(0xffffffffu, cand, o));
-    if (lane == 0 && cand < DBL_MAX)
-      atomicMin(&st->cfl_min_bits, (unsigned long long)__double_as_longlong(cand));
-  }
+  for (int m = 0; m < 5; ++m) S.U[m][c] = u[m];
 }
 
 #endif  // GCS_SWEEPS_TEMPLATES_ONLY

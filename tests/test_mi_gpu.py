@@ -266,3 +266,22 @@ def test_plans_of_different_widths_coexist():
     rc, ref_pot, ref_st = oracle_solve(wide.config, wide.fac, wide.potential)
     assert rc == 0
     check_solution(wide.config, wide.fac, pot, stats[0], ref_pot, ref_st.iterations)
+
+
+@pytest.mark.parametrize("npl,nt", [(361, 181), (192, 22), (600, 12)])
+@pytest.mark.parametrize("iterations", [1, 5, 20])
+def test_first_iterations_follow_the_restatement(npl, nt, iterations):
+    """The recurrence itself, before rounding differences can grow: both
+    solves stopped after the same few iterations (the cap leaves the
+    iterate in the potential) agree to 1e-11 of max|potential|, so a wrong
+    stencil coefficient, alpha or beta shows even where the solve would
+    still converge.  Both launch shapes (column kernel, shared-memory
+    kernel)."""
+    from gamera_cube_b200 import cases
+    case = cases.mi_case(npl, nt, seed=21, max_iterations=iterations)
+    rc, pot, st = gpu_solve(case.config, case.fac, case.potential)
+    ref = oracle_solve(case.config, case.fac, case.potential)
+    assert st.iterations == iterations == ref[2].iterations
+    scale = np.abs(ref[1]).max()
+    assert np.abs(pot - ref[1]).max() <= 1e-11 * scale, np.abs(pot - ref[1]).max() / scale
+    assert abs(st.final_residual - ref[2].final_residual) <= 1e-9 * ref[2].final_residual

@@ -80,3 +80,21 @@ def test_plan_solves_both_hemispheres(lib):
             np.testing.assert_array_equal(got[h], one)
     finally:
         lib.gcs_mi_plan_destroy(plan)
+
+
+@pytest.mark.parametrize("iterations", [1, 5, 20])
+def test_first_iterations_follow_the_restatement(lib, iterations):
+    """The variable-coefficient recurrence stopped after a few iterations
+    equals the restatement's iterate to 1e-11 of its maximum."""
+    c, ped = pedersen_case(361, 181, 3, cases.NORTH)
+    cfg = abi.MiSolverConfig.from_buffer_copy(c.config)
+    cfg.maximum_iterations = iterations
+    dev, sd = c.potential.copy(), abi.MiSolverStats()
+    lib.gcs_mi_solve_pedersen_pcg(C.byref(cfg), c.fac.ctypes.data_as(P),
+                                  ped.ctypes.data_as(P), dev.ctypes.data_as(P), C.byref(sd))
+    cpu, sc = c.potential.copy(), abi.MiSolverStats()
+    oracle_cases.lib().gcso_mi_solve_pedersen_pcg(
+        C.byref(cfg), c.fac.ctypes.data_as(P), ped.ctypes.data_as(P),
+        cpu.ctypes.data_as(P), C.byref(sc))
+    assert sd.iterations == sc.iterations == iterations
+    assert np.abs(dev - cpu).max() <= 1e-11 * np.abs(cpu).max()

@@ -61,8 +61,8 @@ EMF_BYTES_PER_EDGE = 25 * 8
 # (state arrays larger than L2), divided by the faces or edges one launch
 # processes there.  The sweeps stream their arrays, so the traffic of a
 # launch of the bench's workload is these figures times its faces or edges.
-FLUX_TRAFFIC_BYTES_PER_FACE = 354.5
-EMF_TRAFFIC_BYTES_PER_EDGE = 259.4
+FLUX_TRAFFIC_BYTES_PER_FACE = 310.6
+EMF_TRAFFIC_BYTES_PER_EDGE = 277.7
 
 
 def peaks():

@@ -556,6 +556,37 @@ def run_earth(lib, torch, device, args, dist, ctx):
     pc_low, pc_hot = C.c_size_t(), C.c_size_t()
     ok = ok and lib.gcs_context_pressure_control_stats(ctx, C.byref(pc_low), C.byref(pc_hot),
                                                        None, None, 1) == 0
+    # thresholds that make both branches work: from the run's own state, the
+    # low-density threshold at the 30th percentile of the densities, 1.5 c at
+    # the 60th percentile of the sound speeds, the low-density sound speed
+    # half the 10th percentile (the rule of the pressure-control tests)
+    frame = torch.empty(lib.gcs_analysis_frame_floats(ctx), dtype=torch.float32, device=device)
+    ok = ok and lib.gcs_context_analysis_frame(ctx, 5.0 / 3.0, C.c_void_p(frame.data_ptr()),
+                                               None) == 0
+    torch.cuda.synchronize()
+    fv = frame.view(6, 8, -1)
+    rho = fv[:, 0].reshape(-1)[::7].double()
+    cs = torch.sqrt(5.0 / 3.0 * fv[:, 1].reshape(-1)[::7].double() / rho)
+
+    def quantile(x, f):
+        return float(torch.kthvalue(x.cpu(), max(1, int(f * x.numel()))).values)
+
+    pca = abi.PressureControl(5.0 / 3.0, 1e-6, 1e-8, quantile(cs, 0.6) / 1.5,
+                              quantile(rho, 0.3), 0.5 * quantile(cs, 0.1))
+    del frame, fv, rho, cs
+    ok = ok and lib.gcs_context_set_pressure_control(ctx, None, C.byref(pca)) == 0
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    start.record(stream)
+    ok = ok and lib.gcs_context_run_earth(ctx, earth, C.byref(opts), C.byref(ts), 0.5,
+                                          args.earth_steps, 1) == 0
+    stop.record(stream)
+    stop.synchronize()
+    ok = ok and lib.gcs_context_sync(ctx) == 0
+    ms_pca = max_over_ranks(start.elapsed_time(stop), dist, device)
+    pca_low, pca_hot = C.c_size_t(), C.c_size_t()
+    ok = ok and lib.gcs_context_pressure_control_stats(ctx, C.byref(pca_low),
+                                                       C.byref(pca_hot), None, None, 1) == 0
     ok = ok and lib.gcs_context_set_pressure_control(ctx, None, None) == 0
     act = (C.c_size_t * 3)()
     g = C.c_size_t()
@@ -576,7 +607,16 @@ def run_earth(lib, torch, device, args, dist, ctx):
                 "arguments": "gamma 5/3, floors 1e-6/1e-8, c 10, low density 1e-3, "
                              "low-density sound speed 1e-7",
                 "low_density_cells": pc_low.value, "high_sound_speed_cells": pc_hot.value,
-                "gpu_launches_per_step": 24 + 18 + 1}}
+                "gpu_launches_per_step": 24 + 18 + 1,
+                "active": {
+                    "ms_per_step": ms_pca / args.earth_steps,
+                    "arguments": "gamma 5/3, floors 1e-6/1e-8, thresholds from the state: "
+                                 "low density %.4g, c %.4g, low-density sound speed %.4g"
+                                 % (pca.low_density_threshold, pca.light_speed,
+                                    pca.low_density_sound_speed),
+                    "low_density_cells": pca_low.value,
+                    "high_sound_speed_cells": pca_hot.value,
+                    "steps": args.earth_steps}}}
 
 
 ENS_SEED = 2024

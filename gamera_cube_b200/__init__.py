@@ -103,6 +103,8 @@ def _load(path=None):
         "gcs_mi_tensor_plan_upload": (C.c_int, [C.c_void_p] + [P(C.c_double)] * 4),
         "gcs_mi_tensor_solve_async": (C.c_int, [C.c_void_p, C.c_void_p]),
         "gcs_mi_tensor_plan_set_ordering": (C.c_int, [C.c_void_p, C.c_int]),
+        "gcs_mi_tensor_plan_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
+        "gcs_mi_tensor_plan_schedule": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "gcs_mi_tensor_results": (C.c_int, [C.c_void_p, P(abi.MiSolverStats),
                                             P(C.c_int)]),
         "gcs_mi_plan_create": (C.c_int, [P(abi.MiSolverConfig), C.c_int,

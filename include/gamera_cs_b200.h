@@ -668,6 +668,18 @@ int gcs_mi_tensor_solve_async(gcs_mi_tensor_plan *plan, void *stream);
  * swept by the whole cluster at once.  Both solve to the configured
  * tolerance; the iteration counts differ. */
 int gcs_mi_tensor_plan_set_ordering(gcs_mi_tensor_plan *plan, int colored);
+/* Schedule of the row-by-row sweeps (no reference counterpart): 1 the band
+ * pipeline (available where each CTA of the cluster gets at most 32
+ * interior rows and the band's coefficients fit in shared memory; the
+ * default on grids of fewer than 17 longitudes), each CTA sweeping its band
+ * of rows and passing its edge row to the next CTA; 0 one warp advancing
+ * the whole wavefront (the default elsewhere).  Both compute the same
+ * preconditioner with the same operations and give identical results.  -1
+ * when the plan has no band schedule.  gcs_mi_tensor_plan_schedule returns
+ * 1 (band, with the rows per band and the band count), 0 (one warp) or -1. */
+int gcs_mi_tensor_plan_set_schedule(gcs_mi_tensor_plan *plan, int banded);
+int gcs_mi_tensor_plan_schedule(const gcs_mi_tensor_plan *plan, int *rows_per_band,
+                                int *bands);
 int gcs_mi_tensor_results(gcs_mi_tensor_plan *plan, gamera_mi_solver_stats *stats,
                           int *status);
 /* Ionosphere coupling of a device-built case (gcs_context_create_case with

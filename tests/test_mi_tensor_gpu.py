@@ -150,9 +150,10 @@ def test_tensor_rejects_bad_input():
         C.byref(st)) == -1
 
 
-def plan_solve(case, colored):
-    """The device tensor plan with the given SSOR ordering; returns the
-    potential, stats, status and device milliseconds of one solve."""
+def plan_solve(case, colored, banded=None):
+    """The device tensor plan with the given SSOR ordering (and sweep
+    schedule, when given); returns the potential, stats, status and device
+    milliseconds of one solve."""
     import torch
     from gamera_cube_b200 import abi
     L = glib()
@@ -161,6 +162,8 @@ def plan_solve(case, colored):
     assert L.gcs_mi_tensor_plan_create(C.byref(case.config), C.byref(plan)) == 0
     try:
         assert L.gcs_mi_tensor_plan_set_ordering(plan, colored) == 0
+        if banded is not None:
+            assert L.gcs_mi_tensor_plan_set_schedule(plan, banded) == 0
         pot = case.potential.copy()
         assert L.gcs_mi_tensor_plan_upload(plan, ptr(case.fac), ptr(case.pedersen),
                                            ptr(case.hall), ptr(pot)) == 0
@@ -217,3 +220,51 @@ def test_colored_ordering_converges_to_the_reference_solution(npl, nt, hemispher
     assert res <= 2.0 * ref_res, (res, ref_res)
     print("colored %dx%d: %d iterations (reference ordering %d), %.2f ms"
           % (nt, npl, st.iterations, ref_st.iterations, ms))
+
+
+@pytest.mark.parametrize("npl,nt,hemisphere", [
+    (361, 181, 1),   # production grid: 15 bands of 12 rows (the last of 11)
+    (40, 250, -1),   # 16 bands of 16 rows (the last of 8)
+    (12, 70, 1),     # 14 bands of 5 rows (the last of 3)
+    (8, 12, 1),      # 10 rows: 10 bands of one row
+    (17, 60, 1),
+    (5, 40, -1),
+])
+def test_band_schedule_is_bitwise(npl, nt, hemisphere):
+    """The band-pipelined sweeps (each CTA of the cluster sweeps its band of
+    rows; edge rows cross between CTAs through distributed shared memory)
+    against the one-warp wavefront: the same operations on the same
+    operands, so the potential and the stats must agree bit for bit."""
+    from gamera_cube_b200 import cases
+    L = glib()
+    case = cases.mi_case(npl, nt, seed=npl + nt, hemisphere=hemisphere,
+                         max_iterations=20000)
+    plan = C.c_void_p()
+    assert L.gcs_mi_tensor_plan_create(C.byref(case.config), C.byref(plan)) == 0
+    h, n = C.c_int(), C.c_int()
+    try:
+        # the default: bands below 17 longitudes, one warp from 17 on
+        assert L.gcs_mi_tensor_plan_schedule(plan, None, None) == (1 if npl < 17 else 0)
+        assert L.gcs_mi_tensor_plan_set_schedule(plan, 1) == 0
+        assert L.gcs_mi_tensor_plan_schedule(plan, C.byref(h), C.byref(n)) == 1
+        assert L.gcs_mi_tensor_plan_set_schedule(plan, 0) == 0
+        assert L.gcs_mi_tensor_plan_schedule(plan, C.byref(h), C.byref(n)) == 0
+        assert L.gcs_mi_tensor_plan_set_schedule(plan, 2) == -1
+    finally:
+        L.gcs_mi_tensor_plan_destroy(plan)
+    rows = nt - 2
+    assert L.gcs_mi_tensor_plan_create(C.byref(case.config), C.byref(plan)) == 0
+    try:
+        assert L.gcs_mi_tensor_plan_set_schedule(plan, 1) == 0
+        assert L.gcs_mi_tensor_plan_schedule(plan, C.byref(h), C.byref(n)) == 1
+    finally:
+        L.gcs_mi_tensor_plan_destroy(plan)
+    assert h.value == -(-rows // 16) and n.value == -(-rows // h.value)
+    pa, sa, ka, ta = plan_solve(case, 0, banded=0)
+    pb, sb, kb, tb = plan_solve(case, 0, banded=1)
+    assert ka == kb == 0
+    assert (sa.iterations, sa.initial_residual, sa.final_residual, sa.converged) == \
+        (sb.iterations, sb.initial_residual, sb.final_residual, sb.converged)
+    assert np.array_equal(pa, pb)
+    print("band schedule %dx%d: one warp %.2f ms, bands %.2f ms, %d iterations"
+          % (nt, npl, ta, tb, sb.iterations))

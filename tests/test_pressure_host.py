@@ -89,3 +89,5 @@ def test_c_abi_rejects_missing_handles():
     assert lib.gcs_context_set_pressure_control(None, None, C.byref(cfg)) == -1
     assert lib.gcs_context_pressure_control_stats(None, None, None, None, None, 0) == -1
     assert lib.gcs_mi_tensor_plan_set_ordering(None, 1) == -1
+    assert lib.gcs_mi_tensor_plan_set_schedule(None, 1) == -1
+    assert lib.gcs_mi_tensor_plan_schedule(None, None, None) == -1

@@ -226,7 +226,7 @@ __global__ void k_halo_faces(Dims D, const HaloFace *plan, long long count,
 // fused with the CFL time-step reduction of the next step
 // (nonorthogonal_step.c:449-525) over active cells.  mode bit 0: recover
 // and store B; bit 1: CFL reduction (with the stored B when bit 0 is clear).
-__global__ void __launch_bounds__(256) k_recover(Dims D, DevState S, DevGeom G,
+__global__ void __launch_bounds__(256, 4) k_recover(Dims D, DevState S, DevGeom G,
                                                  DevBg BG, Opts O, int mode,
                                                  DevStatus *st) {
   // No early return: every thread reaches the block reduction below.

@@ -118,7 +118,7 @@ __global__ void k_predict(Dims D, DevState S, DevGeom G, Bulk<float> B32, int bu
 template <typename T>
 struct SweepOccupancy {
   static constexpr int flux = 4;
-  static constexpr int edge = 5;
+  static constexpr int edge = 6;
 };
 template <>
 struct SweepOccupancy<float> {

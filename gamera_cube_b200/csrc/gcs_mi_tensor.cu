@@ -22,6 +22,12 @@
 // the reference's (D + L) D^-1 (D + U) with the triangular solves done on
 // D^-1-scaled rows, so it equals the reference's to rounding.
 //
+// Band schedule (the default on grids narrower than 17 longitudes): the
+// same sweeps with the rows split into one band per CTA, each band swept by
+// its CTA's warp 0 from shared-memory tables and its edge row passed to the
+// next CTA through distributed shared memory (band_sweep); identical
+// results.
+//
 // Vector updates, stencil applications and dot products run on all CTAs
 // of the cluster (dot products summed in a fixed order, identical on every
 // CTA); the sweeps run on one warp of CTA 0 between two cluster barriers.

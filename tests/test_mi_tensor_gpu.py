@@ -223,7 +223,7 @@ def test_colored_ordering_converges_to_the_reference_solution(npl, nt, hemispher
 
 
 @pytest.mark.parametrize("npl,nt,hemisphere", [
-    (361, 181, 1),   # production grid: 15 bands of 12 rows (the last of 11)
+    (361, 181, 1),   # production grid: 15 bands of 12 rows on a 16-CTA cluster
     (40, 250, -1),   # 16 bands of 16 rows (the last of 8)
     (12, 70, 1),     # 14 bands of 5 rows (the last of 3)
     (8, 12, 1),      # 10 rows: 10 bands of one row
@@ -259,7 +259,8 @@ def test_band_schedule_is_bitwise(npl, nt, hemisphere):
         assert L.gcs_mi_tensor_plan_schedule(plan, C.byref(h), C.byref(n)) == 1
     finally:
         L.gcs_mi_tensor_plan_destroy(plan)
-    assert h.value == -(-rows // 16) and n.value == -(-rows // h.value)
+    # one band per CTA of the cluster (at most 16), at most 32 rows each
+    assert 1 <= h.value <= 32 and n.value == -(-rows // h.value) and n.value <= 16
     pa, sa, ka, ta = plan_solve(case, 0, banded=0)
     pb, sb, kb, tb = plan_solve(case, 0, banded=1)
     assert ka == kb == 0

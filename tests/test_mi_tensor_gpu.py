@@ -91,6 +91,8 @@ def test_tensor_production_grid():
     (16, 300, -1),  # more than 256 interior rows: 16 chains per lane
     (17, 60, 1),    # the narrowest grid swept 8 diagonals at a time
     (40, 250, -1),  # 8 chains per lane, groups of 8 diagonals
+    (40, 100, 1),   # 4 chains per lane, groups of 8 diagonals
+    (35, 34, -1),   # 1 chain per lane, groups of 8 diagonals
 ])
 def test_tensor_grid_shapes(npl, nt, hemisphere):
     """Every sweep layout (chains per lane, group size) against the oracle.
@@ -229,6 +231,7 @@ def test_colored_ordering_converges_to_the_reference_solution(npl, nt, hemispher
     (8, 12, 1),      # 10 rows: 10 bands of one row
     (17, 60, 1),
     (5, 40, -1),
+    (40, 100, 1),    # one warp with 4 chains per lane
 ])
 def test_band_schedule_is_bitwise(npl, nt, hemisphere):
     """The band-pipelined sweeps (each CTA of the cluster sweeps its band of

@@ -55,11 +55,12 @@ namespace {
 
 // The sweep warp holds 32 M interior colatitude rows (rows padded to
 // Rp = 32 M): M = 1..8 (up to 256 rows) or 16 (up to 512 rows).  It moves
-// diagonals in groups of 8 (a 24-diagonal prefetch ring) where the seam
-// allows (at least 17 longitudes) and shared memory fits, else in groups of
-// 4 (16 diagonals; 8 for M = 16), or of 1 for grids of fewer than 9
-// longitudes: every group pays a fixed synchronisation cost in the sweep
-// warp, so larger groups are faster.
+// diagonals in groups of 12 (a 36-diagonal prefetch ring) where the seam
+// allows (at least 25 longitudes) and shared memory fits (up to 6 chains),
+// else in groups of 8 (24 diagonals; at least 17 longitudes), of 4 (16
+// diagonals; 8 for M = 16), or of 1 for grids of fewer than 9 longitudes:
+// every group pays a fixed synchronisation cost in the sweep warp, so
+// larger groups are faster.
 constexpr int kThreads = 256;
 constexpr int kMaxRows = 512;
 constexpr int kPad = 16;                    // padding diagonals on each side (>= group - 1)
@@ -1164,6 +1165,17 @@ struct Launch {
 };
 
 Launch launch_for(int M, int G) {
+  if (G == 12) {
+    switch (M) {
+      case 1: return {k_tensor<1, 3, 12>, 3, 12};
+      case 2: return {k_tensor<2, 3, 12>, 3, 12};
+      case 3: return {k_tensor<3, 3, 12>, 3, 12};
+      case 4: return {k_tensor<4, 3, 12>, 3, 12};
+      case 5: return {k_tensor<5, 3, 12>, 3, 12};
+      case 6: return {k_tensor<6, 3, 12>, 3, 12};
+      default: return {};
+    }
+  }
   if (G == 8) {
     switch (M) {
       case 1: return {k_tensor<1, 3, 8>, 3, 8};
@@ -1366,7 +1378,10 @@ gcs_mi_tensor_plan *plan_create(const gamera_mi_solver_config *c) {
   S.pot = p->d_pot;
   // (groups of 16 diagonals in a 2-slot ring were tried: 181 x 361 took
   // 470 ms against 192 ms, each group waiting for its whole copy)
-  const int G = !g4 ? 1 : np >= 17 && M <= 8 && tensor_smem(3, 8, Rp, np) <= kSmemCap ? 8 : 4;
+  const int G = !g4 ? 1
+                : np >= 25 && M <= 6 && tensor_smem(3, 12, Rp, np) <= kSmemCap ? 12
+                : np >= 17 && M <= 8 && tensor_smem(3, 8, Rp, np) <= kSmemCap  ? 8
+                                                                                 : 4;
   const Launch L = launch_for(M, G);
   p->kernel = L.kernel;
   p->smem = tensor_smem(L.kRG, L.G, Rp, np);
@@ -1381,7 +1396,7 @@ gcs_mi_tensor_plan *plan_create(const gamera_mi_solver_config *c) {
   // of fewer than 17 longitudes, where the one-warp sweep cannot move its
   // diagonals in groups of 8 and the band pipeline measured faster (B200:
   // 70 x 12 7.5 -> 5.7 ms, 12 x 8 1.3 -> 0.4 ms, 40 x 5 7.6 -> 2.1 ms); on
-  // wider grids the one warp is faster (181 x 361: 192 against 223 ms) and
+  // wider grids the one warp is faster (181 x 361: 163 against 224 ms) and
   // the band schedule is available through gcs_mi_tensor_plan_set_schedule.
   if (p->csize >= 2) {
     const int h = (R + p->csize - 1) / p->csize;
